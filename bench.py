@@ -1,0 +1,443 @@
+"""Benchmark: bit-exact negacyclic products/s at N=32768 with an 868-bit q.
+
+One JSON line on rank 0 (contract of the driver):
+  value      products/s over all ranks with inputs resident in HBM (a step is one
+             pass over a batch of independent products), device-timed;
+  e2e        the same metric through the C ABI's host-buffer call
+             (pm_multiply_host) from pinned host memory: H2D of a, b and D2H of c
+             inside the timed region;
+  roofline   the dominant kernel's algorithmic bytes per launch / its mean
+             device time (CUDA events on its launch stream, recorded by the
+             library during the timed steps);
+  cpu_baseline  the CPU restatement of the reference method (oracle/, all host
+             threads) on a bounded sample of the same workload.
+
+Multi-GPU is replicas only: the method has no exchange step between products,
+so each rank runs its own batch and value sums products over the max-over-
+ranks device time.
+
+--impl reference times the reference's method on the host cores (the oracle
+port: the reference's own path needs cuPQC and a GPU) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "fherma-polymul-baseline_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "bit-exact products/s at N=32768, 868-bit q"
+UNIT = "products/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=32768)
+    ap.add_argument("--bits", type=int, default=868)
+    ap.add_argument("--batch", type=int, default=512, help="independent products per step")
+    ap.add_argument("--e2e-batch", type=int, default=16)
+    ap.add_argument("--tensor", action="store_true", help="tcgen05 INT8 conversion/CRT")
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def seeded_q(seed, bits):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    q = 0
+    for _ in range((bits + 31) // 32):
+        q = (q << 32) | int(rng.integers(0, 2**32))
+    q &= (1 << bits) - 1
+    return q | (1 << (bits - 1)) | 1
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    import datetime
+
+    import torch.distributed as dist
+
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+# ---------------------------------------------------------------------------
+# CPU arms
+# ---------------------------------------------------------------------------
+def cpu_sample(a, b, q, seconds, threads):
+    """Run the oracle port on (a, b) repeatedly for ~seconds; return products/s and count."""
+    from oracle import oracle
+
+    oracle.rns_multiply(a[:64], b[:64], q, threads=threads)  # load + warm
+    done, t0 = 0, time.perf_counter()
+    while True:
+        oracle.rns_multiply(a, b, q, threads=threads)
+        done += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            return done / el, done, el
+
+
+def host_inputs(n, q, seed, count=1):
+    import numpy as np
+
+    from tests.helpers import uniform_below
+
+    rng = np.random.default_rng(seed)
+    limbs = (q.bit_length() + 63) // 64
+    return [(uniform_below(rng, q, n, limbs), uniform_below(rng, q, n, limbs)) for _ in range(count)]
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    q = seeded_q(args.seed, args.bits)
+    (a, b), = host_inputs(args.n, q, args.seed + 1)
+    from oracle import oracle
+
+    for _ in range(max(args.warmup, 1)):
+        oracle.rns_multiply(a, b, q, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.rns_multiply(a, b, q, threads=threads)
+    el = time.perf_counter() - t0
+    value = args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"one negacyclic product per step, N={args.n}, {args.bits}-bit seeded odd q, "
+                               "coefficients uniform in [0, q)", "n": args.n, "q_bits": args.bits,
+                   "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} products at N={args.n}; the reference's RNS method restated in C "
+                                   "(oracle/polymul_oracle.c), threads over primes; the reference's own path "
+                                   "needs cuPQC and a GPU"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid):
+        self.uuid = device_uuid
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "50"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, f[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def device_inputs(torch, batch, n, limbs, q, seed):
+    """Seeded coefficients uniform in [0, q) generated on the device by rejection."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    bits = q.bit_length()
+    top = bits - 64 * (limbs - 1)
+    q_limbs = [(q >> (64 * j)) & ((1 << 64) - 1) for j in range(limbs)]
+    sign = -(1 << 63)
+
+    def order_key(v):  # an unsigned limb as the int64 that sorts the same way
+        s = v ^ (1 << 63)
+        return s - (1 << 64) if s >= (1 << 63) else s
+
+    q_s = torch.tensor([order_key(v) for v in q_limbs], dtype=torch.int64, device="cuda")
+
+    def draw(rows):
+        hi = torch.randint(0, 2**32, (rows, n, limbs), dtype=torch.int64, device="cuda", generator=g)
+        lo = torch.randint(0, 2**32, (rows, n, limbs), dtype=torch.int64, device="cuda", generator=g)
+        x = (hi << 32) | lo
+        x[..., limbs - 1] &= (1 << top) - 1 if top < 64 else -1
+        return x
+
+    out = draw(batch)
+    for _ in range(64):
+        xs = out ^ sign  # unsigned order as signed order
+        less = torch.zeros(out.shape[:2], dtype=torch.bool, device="cuda")
+        equal = torch.ones_like(less)
+        for j in range(limbs - 1, -1, -1):
+            less |= equal & (xs[..., j] < q_s[j])
+            equal &= xs[..., j] == q_s[j]
+        bad = ~less
+        nbad = int(bad.sum())
+        if nbad == 0:
+            return out
+        fresh = draw(1).reshape(n, limbs)
+        while fresh.shape[0] < nbad:
+            fresh = torch.cat([fresh, draw(1).reshape(n, limbs)])
+        out[bad] = fresh[:nbad]
+    raise RuntimeError("rejection sampling did not converge")
+
+
+def algorithmic_bytes(n, primes, limbs):
+    """Mandatory HBM bytes per launch of each kernel for one product."""
+    io = n * 8 * limbs
+    return {
+        "k1_convert_cols": 2 * io + 2 * primes * n * 4,
+        "k2_rows": 2 * primes * n * 4 + primes * n * 4,
+        "k3_cols_crt": primes * n * 4 + io,
+    }
+
+
+def read_profile_traffic(kernel):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import polymul
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(world, "nccl")
+    n, bits = args.n, args.bits
+    q = seeded_q(args.seed, bits)
+    limbs = (bits + 63) // 64
+    plan = polymul.Plan(n, q, coef_limbs=limbs, tensor=args.tensor)
+    B = args.batch
+    A = device_inputs(torch, B, n, limbs, q, args.seed + 17 + 1000 * rank)
+    Bv = device_inputs(torch, B, n, limbs, q, args.seed + 29 + 1000 * rank)
+    Cv = torch.empty_like(A)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    def step():
+        for k in range(B):
+            plan.multiply(A[k].data_ptr(), Bv[k].data_ptr(), Cv[k].data_ptr(), 0, sh)
+
+    # bit-exact check of sampled products against the oracle (outside the timed region)
+    from oracle import oracle
+
+    step()
+    stream.synchronize()
+    mismatches, checked = 0, 0
+    for k in sorted({0, B // 2, B - 1}):
+        a = A[k].cpu().numpy().view(np.uint64)
+        b = Bv[k].cpu().numpy().view(np.uint64)
+        c = Cv[k].cpu().numpy().view(np.uint64)
+        mismatches += int((oracle.rns_multiply(a, b, q) != c).any(axis=1).sum())
+        checked += 1
+    if mismatches:
+        raise SystemExit(f"bench aborted: {mismatches} mismatching coefficients against the oracle")
+
+    for _ in range(max(args.warmup - 1, 0)):
+        step()
+    stream.synchronize()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    polymul.profile_enable(3 * B * args.steps + 16)
+    launches0 = polymul.launch_count()
+    sampler.start()
+    time.sleep(0.1)  # let the sampler attach before the timed region
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    clocks = sampler.stop()
+    launches = polymul.launch_count() - launches0
+    prof = polymul.profile_read()
+    polymul.profile_enable(0)
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_products = B * args.steps * world
+    value = total_products / (ms / 1000.0)
+
+    # end to end through the C ABI host-buffer call, pinned host memory
+    E = min(args.e2e_batch, B)
+    ha = torch.empty((E, n, limbs), dtype=torch.int64, pin_memory=True)
+    hb = torch.empty_like(ha, pin_memory=True)
+    hc = torch.empty_like(ha, pin_memory=True)
+    ha.copy_(A[:E])
+    hb.copy_(Bv[:E])
+    del A, Bv, Cv
+    torch.cuda.empty_cache()
+    lib = polymul.lib()
+
+    def e2e_step():
+        for k in range(E):
+            polymul.check(lib.pm_multiply_host(plan.handle, ha[k].data_ptr(), hb[k].data_ptr(), hc[k].data_ptr()))
+
+    for _ in range(max(args.warmup, 1)):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = E * args.steps * world / e2e_s
+    io = n * 8 * limbs
+
+    # roofline of the dominant kernel
+    alg = algorithmic_bytes(n, plan.primes, limbs)
+    dom = max(prof, key=lambda k: prof[k][1]) if prof else None
+    roofline = None
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peak_src = "measured"
+    kernels = {}
+    for name, (cnt, tot) in prof.items():
+        mean_ms = tot / cnt
+        gbs = alg.get(name, 0) / (mean_ms / 1000.0) / 1e9 if name in alg else None
+        kernels[name] = {"launches": cnt, "mean_us": 1000 * mean_ms, "share": tot / sum(v[1] for v in prof.values()),
+                         "achieved_gbs": gbs}
+    if dom:
+        cnt, tot = prof[dom]
+        achieved = alg[dom] / (tot / cnt / 1000.0) / 1e9
+        traffic = read_profile_traffic(dom)
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                    "algorithmic_bytes_per_launch": alg[dom]}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        (ca, cb), = host_inputs(n, q, args.seed + 5)
+        threads = os.cpu_count() or 1
+        v, done, el = cpu_sample(ca, cb, q, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{done} products (N={n}, {bits}-bit q) in {el:.1f} s through the C restatement of the "
+                         "reference RNS method (oracle/polymul_oracle.c), threads over primes"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"batch of {B} independent negacyclic products per step, N={n}, {bits}-bit "
+                                   f"seeded odd q, coefficients uniform in [0, q) generated on the device",
+                       "n": n, "q_bits": bits, "batch": B, "primes": plan.primes,
+                       "path": "tensor" if args.tensor else "simt",
+                       "l2": f"inputs larger than L2: {2 * B * io / 1e9:.2f} GB of a, b read per step",
+                       "parallelism": f"replicas x{world}", "oracle_check": f"{checked} products bit-exact"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * E * io, "d2h_bytes_per_step": E * io,
+                    "api": "pm_multiply_host, pinned host buffers", "products_per_step": E},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "mismatches": mismatches,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        world, _, _ = dist_env()
+        return
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

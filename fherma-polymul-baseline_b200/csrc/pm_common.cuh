@@ -1,0 +1,62 @@
+// Constants and modular arithmetic shared by the device kernels and the host
+// code that prepares their tables.
+#pragma once
+
+#include <cstdint>
+
+namespace pm {
+
+constexpr int kLogNMax = 16;
+constexpr int kNMax = 1 << kLogNMax;  // largest ring dimension; twiddle tables are this long
+constexpr int kPMax = 64;             // largest prime basis
+constexpr int kWMax = 28;             // largest q in 32-bit words (896 bits)
+constexpr int kPowWords = 32;         // rows of 2^(32k) mod p kept per prime
+
+struct PrimeConst {
+    uint32_t p;
+    uint32_t two_p;
+    uint32_t mu;    // floor(2^61 / p), p in (2^29, 2^30)
+    uint32_t pad;
+    uint64_t recip; // floor(2^64 / p)
+};
+
+// x * w mod p up to one extra p: result in [0, 2p) for any 32-bit x.
+// w = (value, floor(value * 2^32 / p)).
+__device__ __forceinline__ uint32_t shoup_mul(uint32_t x, uint2 w, uint32_t p) {
+    return x * w.x - __umulhi(x, w.y) * p;
+}
+
+// [0, 2m) -> [0, m); the unsigned min picks x - m exactly when it did not wrap.
+__device__ __forceinline__ uint32_t csub(uint32_t x, uint32_t m) { return min(x, x - m); }
+
+// x mod p for x < 2^60 (Barrett with mu = floor(2^61/p)); quotient error <= 2.
+__device__ __forceinline__ uint32_t reduce60(uint64_t x, uint32_t p, uint32_t mu) {
+    uint32_t xh = uint32_t(x >> 29);
+    uint32_t q = uint32_t((uint64_t(xh) * mu) >> 32);
+    uint32_t r = uint32_t(x) - q * p;
+    r = csub(r, p);
+    return csub(r, p);
+}
+
+// Forward Cooley-Tukey butterfly, Harvey lazy: x, y in [0, 4p) -> [0, 4p).
+__device__ __forceinline__ void ct_bfly(uint32_t& x, uint32_t& y, uint2 w, uint32_t p, uint32_t two_p) {
+    uint32_t xr = csub(x, two_p);
+    uint32_t t = shoup_mul(y, w, p);
+    x = xr + t;
+    y = xr - t + two_p;
+}
+
+// Inverse Gentleman-Sande butterfly, Harvey lazy: x, y in [0, 2p) -> [0, 2p).
+__device__ __forceinline__ void gs_bfly(uint32_t& x, uint32_t& y, uint2 w, uint32_t p, uint32_t two_p) {
+    uint32_t s = x + y;
+    uint32_t d = x - y + two_p;
+    x = csub(s, two_p);
+    y = shoup_mul(d, w, p);
+}
+
+// Shared-memory swizzle: an XOR of index bits 4..7 into bits 1..4.  It is a
+// bijection on every aligned power-of-two range and keeps the strided row
+// passes of K2 free of bank conflicts.
+__device__ __forceinline__ int swz(int idx) { return idx ^ (((idx >> 4) & 0xF) << 1); }
+
+}  // namespace pm

@@ -1,0 +1,438 @@
+// Device arithmetic and the three fused passes of one negacyclic product.
+//
+//   K1 convert_cols : wide coefficients -> residues mod every prime, then the
+//                     first log2(R) forward NTT stages ("column" stages, whose
+//                     butterflies span the R rows of an R x C view) done across
+//                     the lanes of a warp.
+//   K2 rows         : per (prime, row): the remaining forward stages of a and
+//                     b in registers + shared memory, the pointwise product,
+//                     and the first inverse stages -- one HBM read of a, b and
+//                     one write of the product per row.
+//   K3 cols_crt     : the last inverse stages across warp lanes, the CRT digit
+//                     t_i = r_i * N^-1 * (P/p_i)^-1, exact CRT accumulation,
+//                     fixed-point nearest quotient and the reduction mod q.
+//
+// The reference runs the same algebra as nine kernels per product
+// (rns/solve.cu:128-420: transpose_inputs, prepare_rns, reverse_rns,
+// small_rns x2, fused_tail_rns x2, product_rns, reconstruct_rns).  Its
+// psi-twist tables are replaced by psi-merged twiddles (research/
+// negacyclic_order.py ordering), which need no twist pass and let one
+// bit-reversed twiddle table per prime serve every N <= 65536 as a prefix.
+//
+// Lazy ranges (Harvey): forward values stay in [0, 4p), inverse values in
+// [0, 2p); primes are below 2^30 so 4p fits a 32-bit word.
+#pragma once
+
+#include <cstdint>
+
+#include "pm_common.cuh"
+
+namespace pm {
+
+// ---------------------------------------------------------------------------
+// K1: conversion + forward column stages (plain SIMT conversion).
+// grid (C/G, 2), block R*G threads; thread (g, r) owns coefficient r*C + col0 + g.
+// ---------------------------------------------------------------------------
+template <int W>
+__global__ void __launch_bounds__(256) k1_convert_cols(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                                       uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
+                                                       const uint2* __restrict__ conv_pow,
+                                                       const uint2* __restrict__ tw_fwd, int n, int logR, int logC,
+                                                       int P, int stride) {
+    __shared__ uint32_t tile[256];
+    const int R = 1 << logR;
+    const int G = blockDim.x >> logR;
+    const int r = threadIdx.x & (R - 1), g = threadIdx.x >> logR;
+    const int col0 = blockIdx.x * G;
+    const size_t J = (size_t(r) << logC) + col0 + g;
+    const uint32_t* src = (blockIdx.y ? b : a) + J * stride;
+    uint32_t x[W];
+#pragma unroll
+    for (int k = 0; k < W; k += 2) {
+        uint2 v = make_uint2(0, 0);
+        if (k < stride) v = __ldg(reinterpret_cast<const uint2*>(src + k));
+        x[k] = v.x;
+        x[k + 1] = v.y;
+    }
+    const unsigned mask = blockDim.x >= 32 ? 0xffffffffu : ((1u << blockDim.x) - 1);
+    uint32_t* dst = res + size_t(blockIdx.y) * P * n;
+    const int t = threadIdx.x, tr = t / G, tg = t % G;
+    for (int i = 0; i < P; ++i) {
+        const PrimeConst pc = pcs[i];
+        const uint2* cp = conv_pow + i * kPowWords;
+        uint64_t acc = 0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) acc += shoup_mul(x[k], __ldg(cp + k), pc.p);
+        uint32_t v = reduce60(acc, pc.p, pc.mu);
+        const uint2* tw = tw_fwd + size_t(i) * kNMax;
+        for (int s = 0; s < logR; ++s) {
+            const int bit = logR - 1 - s;
+            const bool upper = (r >> bit) & 1;
+            const uint2 w = __ldg(tw + (1 << s) + (r >> (logR - s)));
+            const uint32_t send = upper ? shoup_mul(v, w, pc.p) : csub(v, pc.two_p);
+            const uint32_t recv = __shfl_xor_sync(mask, send, 1 << bit);
+            v = upper ? recv - send + pc.two_p : send + recv;
+        }
+        __syncthreads();
+        tile[r * G + g] = v;
+        __syncthreads();
+        dst[size_t(i) * n + (size_t(tr) << logC) + col0 + tg] = tile[t];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2: row stages.  Element mapping of a pass over stages s0..s0+K-1 of a row
+// of C = 2^LOGC values, 8 values per thread, T = C/8 threads per row:
+//   d = C >> (s0+K); for group m < 8>>K: gid = tid + T*m, blk = gid / d,
+//   o = gid % d; value l of the group sits at blk*(d<<K) + o + l*d.
+// Forward twiddle of stage s = s0+u for the value pair starting at l:
+//   Psi_rev[(R + r) * 2^s + blk * 2^u + (l >> (K-u))].
+// ---------------------------------------------------------------------------
+template <int K>
+__device__ __forceinline__ int pass_index(int tid, int T, int m, int l, int logd) {
+    const int gid = tid + T * m;
+    const int blk = gid >> logd;
+    const int o = gid & ((1 << logd) - 1);
+    return (blk << (logd + K)) + o + (l << logd);
+}
+
+template <int K>
+__device__ __forceinline__ void pass_store(const uint32_t (&v)[8], uint32_t* s, int tid, int T, int logd) {
+#pragma unroll
+    for (int m = 0; m < (8 >> K); ++m)
+#pragma unroll
+        for (int l = 0; l < (1 << K); ++l) s[swz(pass_index<K>(tid, T, m, l, logd))] = v[(m << K) + l];
+}
+
+template <int K>
+__device__ __forceinline__ void pass_load(uint32_t (&v)[8], const uint32_t* s, int tid, int T, int logd) {
+#pragma unroll
+    for (int m = 0; m < (8 >> K); ++m)
+#pragma unroll
+        for (int l = 0; l < (1 << K); ++l) v[(m << K) + l] = s[swz(pass_index<K>(tid, T, m, l, logd))];
+}
+
+template <int K>
+__device__ __forceinline__ void pass_forward(uint32_t (&va)[8], uint32_t (&vb)[8], int tid, int T, int s0, int logd,
+                                             int rowbase, const uint2* __restrict__ tw, uint32_t p, uint32_t two_p) {
+#pragma unroll
+    for (int m = 0; m < (8 >> K); ++m) {
+        const int blk = (tid + T * m) >> logd;
+#pragma unroll
+        for (int u = 0; u < K; ++u) {
+            const int h = 1 << (K - 1 - u);
+            const uint2* tws = tw + ((rowbase << (s0 + u)) + (blk << u));
+#pragma unroll
+            for (int l = 0; l < (1 << K); ++l) {
+                if (l & h) continue;
+                const uint2 w = __ldg(tws + (l >> (K - u)));
+                ct_bfly(va[(m << K) + l], va[(m << K) + l + h], w, p, two_p);
+                ct_bfly(vb[(m << K) + l], vb[(m << K) + l + h], w, p, two_p);
+            }
+        }
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, int s0, int logd, int rowbase,
+                                             const uint2* __restrict__ tw, uint32_t p, uint32_t two_p) {
+#pragma unroll
+    for (int m = 0; m < (8 >> K); ++m) {
+        const int blk = (tid + T * m) >> logd;
+#pragma unroll
+        for (int u = K - 1; u >= 0; --u) {
+            const int h = 1 << (K - 1 - u);
+            const uint2* tws = tw + ((rowbase << (s0 + u)) + (blk << u));
+#pragma unroll
+            for (int l = 0; l < (1 << K); ++l) {
+                if (l & h) continue;
+                const uint2 w = __ldg(tws + (l >> (K - u)));
+                gs_bfly(v[(m << K) + l], v[(m << K) + l + h], w, p, two_p);
+            }
+        }
+    }
+}
+
+// Rows of C = 2^LOGC >= 8.  grid (R / rows_per_cta, P), block rows_per_cta * C/8.
+// Dynamic shared memory: rows_per_cta * 2 * C words.  The product overwrites
+// the a plane in place.
+template <int LOGC>
+__global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
+                                               const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv,
+                                               int n, int logR, int P) {
+    constexpr int C = 1 << LOGC;
+    constexpr int T = C / 8;
+    constexpr int NP3 = LOGC / 3;  // radix-8 passes
+    constexpr int REM = LOGC % 3;  // stages of the closing pass
+    extern __shared__ uint32_t smem[];
+    const int sub = threadIdx.x / T, tid = threadIdx.x % T;
+    const int rows_per_cta = blockDim.x / T;
+    const int r = blockIdx.x * rows_per_cta + sub;
+    const int i = blockIdx.y;
+    const int R = 1 << logR;
+    uint32_t* sa = smem + sub * 2 * C;
+    uint32_t* sb = sa + C;
+    const PrimeConst pc = pcs[i];
+    uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
+    const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
+    const uint2* twf = tw_fwd + size_t(i) * kNMax;
+    const uint2* twi = tw_inv + size_t(i) * kNMax;
+    const int rowbase = R + r;
+
+    uint32_t va[8], vb[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        va[l] = ga[tid + l * T];
+        vb[l] = gb[tid + l * T];
+    }
+    // forward radix-8 passes
+#pragma unroll
+    for (int q3 = 0; q3 < NP3; ++q3) {
+        const int s0 = 3 * q3, logd = LOGC - s0 - 3;
+        if (q3 > 0) {
+            pass_load<3>(va, sa, tid, T, logd);
+            pass_load<3>(vb, sb, tid, T, logd);
+        }
+        pass_forward<3>(va, vb, tid, T, s0, logd, rowbase, twf, pc.p, pc.two_p);
+        if (q3 + 1 < NP3 || REM) {
+            __syncthreads();
+            pass_store<3>(va, sa, tid, T, logd);
+            pass_store<3>(vb, sb, tid, T, logd);
+            __syncthreads();
+        }
+    }
+    if constexpr (REM > 0) {
+        const int s0 = 3 * NP3, logd = 0;
+        pass_load<REM>(va, sa, tid, T, logd);
+        pass_load<REM>(vb, sb, tid, T, logd);
+        pass_forward<REM>(va, vb, tid, T, s0, logd, rowbase, twf, pc.p, pc.two_p);
+    }
+    // pointwise product, operands reduced to [0, p)
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const uint32_t x = csub(csub(va[l], pc.two_p), pc.p);
+        const uint32_t y = csub(csub(vb[l], pc.two_p), pc.p);
+        va[l] = reduce60(uint64_t(x) * y, pc.p, pc.mu);
+    }
+    if constexpr (REM > 0) {
+        const int s0 = 3 * NP3, logd = 0;
+        pass_inverse<REM>(va, tid, T, s0, logd, rowbase, twi, pc.p, pc.two_p);
+        __syncthreads();
+        pass_store<REM>(va, sa, tid, T, logd);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q3 = NP3 - 1; q3 >= 0; --q3) {
+        const int s0 = 3 * q3, logd = LOGC - s0 - 3;
+        if (q3 + 1 < NP3 || REM) pass_load<3>(va, sa, tid, T, logd);
+        pass_inverse<3>(va, tid, T, s0, logd, rowbase, twi, pc.p, pc.two_p);
+        if (q3 > 0) {
+            __syncthreads();
+            pass_store<3>(va, sa, tid, T, logd);
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int l = 0; l < 8; ++l) ga[tid + l * T] = va[l];
+}
+
+// Rows of C <= 4 (N <= 128): one thread per row, everything in registers.
+__global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
+                              const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv, int n, int logR,
+                              int logC, int P) {
+    const int R = 1 << logR, C = 1 << logC;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (r >= R) return;
+    const PrimeConst pc = pcs[i];
+    uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
+    const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
+    const uint2* twf = tw_fwd + size_t(i) * kNMax;
+    const uint2* twi = tw_inv + size_t(i) * kNMax;
+    uint32_t va[4], vb[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        va[j] = j < C ? ga[j] : 0;
+        vb[j] = j < C ? gb[j] : 0;
+    }
+    for (int s = 0; s < logC; ++s) {
+        const int t = C >> (s + 1);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j < C && !(j & t)) {
+                const uint2 w = twf[((R + r) << s) + (j >> (logC - s))];
+                // indices are compile-time after unrolling; t is runtime, select explicitly
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (k == j + t) {
+                        ct_bfly(va[j], va[k], w, pc.p, pc.two_p);
+                        ct_bfly(vb[j], vb[k], w, pc.p, pc.two_p);
+                    }
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t x = csub(csub(va[j], pc.two_p), pc.p);
+        const uint32_t y = csub(csub(vb[j], pc.two_p), pc.p);
+        va[j] = reduce60(uint64_t(x) * y, pc.p, pc.mu);
+    }
+    for (int s = logC - 1; s >= 0; --s) {
+        const int t = C >> (s + 1);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j < C && !(j & t)) {
+                const uint2 w = twi[((R + r) << s) + (j >> (logC - s))];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (k == j + t) gs_bfly(va[j], va[k], w, pc.p, pc.two_p);
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (j < C) ga[j] = va[j];
+}
+
+// ---------------------------------------------------------------------------
+// Multiprecision tail of the CRT, per coefficient, all in registers.
+// acc: W+2 columns of 64-bit deferred-carry sums.
+// ---------------------------------------------------------------------------
+template <int W>
+__device__ __forceinline__ void normalize(uint64_t (&acc)[W + 2]) {
+    uint64_t carry = 0;
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        const uint64_t v = acc[k] + carry;
+        acc[k] = v & 0xffffffffull;
+        carry = v >> 32;
+    }
+}
+
+// v (W+2 words) mod q, v < 2^(sbits+37); q has sbits bits and W words;
+// mu_q = floor(2^(sbits+62) / q).  Writes W words of the canonical residue.
+template <int W>
+__device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q, uint64_t mu_q,
+                                             int sbits) {
+    // X = floor(v / 2^(sbits-1)), < 2^38
+    const int sh = sbits - 1;
+    uint64_t X = 0;
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        const int pos = 32 * k - sh;  // bit position of word k inside X
+        if (pos > -32 && pos < 64) X |= pos >= 0 ? uint64_t(v[k]) << pos : uint64_t(v[k]) >> (-pos);
+    }
+    const uint64_t hi = __umul64hi(X, mu_q), lo = X * mu_q;
+    const uint64_t Q = (hi << 1) | (lo >> 63);
+    const uint32_t qlo = uint32_t(Q), qhi = uint32_t(Q >> 32);
+    // v -= Q * q, computed as q*qlo + (q*qhi << 32)
+    uint32_t t[W + 2];
+    uint64_t c1 = 0, c2 = 0;
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        const uint64_t a1 = (k < W ? uint64_t(q[k]) * qlo : 0) + c1;
+        c1 = a1 >> 32;
+        const uint64_t a2 = (k >= 1 && k - 1 < W ? uint64_t(q[k - 1]) * qhi : 0) + uint32_t(a1) + c2;
+        c2 = a2 >> 32;
+        t[k] = uint32_t(a2);
+    }
+    uint32_t borrow = 0;
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        const uint64_t d = uint64_t(v[k]) - t[k] - borrow;
+        v[k] = uint32_t(d);
+        borrow = uint32_t(d >> 63);
+    }
+    // two conditional subtractions bring [0, 3q) to [0, q)
+#pragma unroll
+    for (int rep = 0; rep < 2; ++rep) {
+        uint32_t d[W + 2];
+        uint32_t br = 0;
+#pragma unroll
+        for (int k = 0; k < W + 2; ++k) {
+            const uint64_t x = uint64_t(v[k]) - (k < W ? q[k] : 0) - br;
+            d[k] = uint32_t(x);
+            br = uint32_t(x >> 63);
+        }
+#pragma unroll
+        for (int k = 0; k < W + 2; ++k) v[k] = br ? v[k] : d[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K3: inverse column stages + CRT (plain SIMT accumulation).
+// grid (C/G), block R*G; dynamic shared memory P*W words ((P/p_i) mod q rows).
+// consts = q[W] followed by (-P mod q)[W].
+// ---------------------------------------------------------------------------
+template <int W>
+__global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
+                                                   const PrimeConst* __restrict__ pcs,
+                                                   const uint2* __restrict__ tw_inv, const uint2* __restrict__ scale,
+                                                   const uint32_t* __restrict__ mq,
+                                                   const uint32_t* __restrict__ consts, uint64_t mu_q, int sbits,
+                                                   int n, int logR, int logC, int P, int stride) {
+    extern __shared__ uint32_t s_mq[];
+    __shared__ uint32_t tile[256];
+    __shared__ uint32_t s_q[2 * W];
+    for (int k = threadIdx.x; k < P * W; k += blockDim.x) s_mq[k] = mq[k];
+    for (int k = threadIdx.x; k < 2 * W; k += blockDim.x) s_q[k] = consts[k];
+    const int R = 1 << logR;
+    const int G = blockDim.x >> logR;
+    const int r = threadIdx.x & (R - 1), g = threadIdx.x >> logR;
+    const int col0 = blockIdx.x * G;
+    const int t = threadIdx.x, tr = t / G, tg = t % G;
+    const unsigned mask = blockDim.x >= 32 ? 0xffffffffu : ((1u << blockDim.x) - 1);
+    uint64_t acc[W + 2];
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) acc[k] = 0;
+    uint64_t f0 = 0, f1 = 0;
+    for (int i = 0; i < P; ++i) {
+        __syncthreads();
+        tile[t] = res[size_t(i) * n + (size_t(tr) << logC) + col0 + tg];
+        __syncthreads();
+        uint32_t v = tile[r * G + g];
+        const PrimeConst pc = pcs[i];
+        const uint2* tw = tw_inv + size_t(i) * kNMax;
+        for (int s = logR - 1; s >= 0; --s) {
+            const int bit = logR - 1 - s;
+            const bool upper = (r >> bit) & 1;
+            const uint32_t other = __shfl_xor_sync(mask, v, 1 << bit);
+            if (!upper) {
+                v = csub(v + other, pc.two_p);
+            } else {
+                const uint2 w = __ldg(tw + (1 << s) + (r >> (logR - s)));
+                v = shoup_mul(other - v + pc.two_p, w, pc.p);
+            }
+        }
+        const uint32_t ti = csub(shoup_mul(v, __ldg(scale + i), pc.p), pc.p);
+        const uint32_t* m = s_mq + i * W;
+#pragma unroll
+        for (int k = 0; k < W; ++k) acc[k] += uint64_t(ti) * m[k];
+        f0 += uint64_t(ti) * uint32_t(pc.recip);
+        f1 += uint64_t(ti) * uint32_t(pc.recip >> 32);
+        if ((i & 3) == 3) {
+            normalize<W>(acc);
+            f1 += f0 >> 32;
+            f0 &= 0xffffffffull;
+        }
+    }
+    normalize<W>(acc);
+    f1 += f0 >> 32;
+    // nearest integer of sum t_i / p_i  (fraction carried in f1:f0 / 2^64)
+    const uint32_t nearest = uint32_t((f1 + (1ull << 31)) >> 32);
+    uint32_t v[W + 2];
+    uint64_t carry = 0;
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        const uint64_t x = acc[k] + (k < W ? uint64_t(s_q[W + k]) * nearest : 0) + carry;
+        v[k] = uint32_t(x);
+        carry = x >> 32;
+    }
+    reduce_mod_q<W>(v, s_q, mu_q, sbits);
+    const size_t J = (size_t(r) << logC) + col0 + g;
+    uint32_t* dst = out + J * stride;
+#pragma unroll
+    for (int k = 0; k < W; k += 2)
+        if (k < stride) *reinterpret_cast<uint2*>(dst + k) = make_uint2(v[k], v[k + 1]);
+    for (int k = W; k < stride; ++k) dst[k] = 0;
+}
+
+}  // namespace pm

@@ -1,0 +1,94 @@
+// Internal types shared by the host translation units of libpolymul.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "host_math.h"
+#include "pm_common.cuh"
+
+namespace pm {
+
+struct Failure : std::runtime_error {
+    int status;
+    Failure(int s, std::string m);
+};
+
+void cuda_check(cudaError_t e, const char* what);
+int fail(int status, const std::string& message);
+void count_launches(uint64_t k);
+
+// Records a CUDA event pair around the launches in its scope while
+// pm_profile_enable is on; a no-op otherwise.
+struct ProfileScope {
+    cudaStream_t stream;
+    long index = -1;
+    ProfileScope(const char* name, cudaStream_t st);
+    ~ProfileScope();
+};
+int profile_enable(uint32_t capacity);
+int profile_read(const char** names, uint64_t* launches, double* total_ms, uint32_t capacity, uint32_t* count);
+
+// Device-resident prime basis shared by every plan on one GPU.
+struct DeviceBasis {
+    int device = 0;
+    std::vector<uint32_t> primes;   // kPMax primes, descending
+    PrimeConst* d_pc = nullptr;     // [kPMax]
+    uint2* d_tw_fwd = nullptr;      // [kPMax][kNMax] psi^brev(k)   (value, Shoup)
+    uint2* d_tw_inv = nullptr;      // [kPMax][kNMax] psi^-brev(k)
+    uint2* d_conv_pow = nullptr;    // [kPMax][kPowWords] 2^(32k) mod p
+    // tensor-core conversion table (built on first tensor plan)
+    uint8_t* d_conv_weights = nullptr;
+    ~DeviceBasis();
+};
+
+DeviceBasis& basis_for_device(int device);
+std::vector<uint32_t> make_primes();
+unsigned basis_size(const std::vector<uint32_t>& primes, unsigned n, unsigned qbits);
+
+// Everything one (n, q) product needs on the device.
+struct PlanCore {
+    int device = 0;
+    uint32_t n = 0, logn = 0, logR = 0, logC = 0;
+    uint32_t P = 0;          // basis size
+    uint32_t qbits = 0;
+    uint32_t W = 0;          // q words rounded up to a multiple of 4 (kernel template width)
+    uint32_t coef_limbs = 0, stride = 0;  // u64 limbs and u32 words per coefficient
+    uint32_t flags = 0;
+    Words q;
+    uint64_t mu_q = 0;
+    DeviceBasis* basis = nullptr;
+    uint32_t* d_mq = nullptr;      // [P][W] (P_total/p_i) mod q
+    uint32_t* d_consts = nullptr;  // q[W], (-P_total mod q)[W]
+    uint2* d_scale = nullptr;      // [P] n^-1 (P_total/p_i)^-1 mod p_i
+    uint32_t* d_work = nullptr;    // [2][P][n] residue planes (plan-owned workspace)
+    size_t workspace_bytes = 0;
+    size_t io_bytes = 0;           // bytes of one polynomial
+    void* d_io = nullptr;          // a, b, c device copies for the host-buffer call
+    void* h_stage = nullptr;       // pinned staging for pageable host buffers
+    cudaStream_t stream = nullptr;
+    // tensor path constants
+    uint8_t* d_crt_weights = nullptr;
+    uint32_t tensor_k_crt = 0;
+
+    void init(uint32_t n, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs, uint32_t flags);
+    ~PlanCore();
+};
+
+void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
+                 cudaStream_t st);
+void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
+                    cudaStream_t st);
+void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c);
+
+// tensor-core conversion / CRT (tensor.cu)
+void tensor_init(PlanCore& s);
+void tensor_release(PlanCore& s);
+void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
+                   cudaStream_t st);
+
+}  // namespace pm

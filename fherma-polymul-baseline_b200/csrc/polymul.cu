@@ -1,0 +1,587 @@
+// Host side of the multiplier: the per-device prime basis, plans, the launch
+// sequence of one product, and the C ABI declared in include/polymul.h.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/polymul.h"
+#include "host_math.h"
+#include "pm_device.cuh"
+#include "pm_internal.h"
+
+namespace pm {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0};
+
+Failure::Failure(int s, std::string m) : std::runtime_error(m), status(s) {}
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Failure(PM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void count_launches(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+// ---------------------------------------------------------------------------
+// kernel timing (pm_profile_*)
+// ---------------------------------------------------------------------------
+namespace {
+struct ProfileRecord {
+    const char* name;
+    cudaEvent_t start, stop;
+};
+std::mutex g_prof_mutex;
+std::atomic<bool> g_prof_on{false};
+std::vector<cudaEvent_t> g_prof_pool;
+std::vector<ProfileRecord> g_prof_pending;
+size_t g_prof_used = 0;
+struct ProfileTotal {
+    const char* name;
+    uint64_t launches;
+    double ms;
+};
+std::vector<ProfileTotal> g_prof_totals;
+}  // namespace
+
+ProfileScope::ProfileScope(const char* name, cudaStream_t st) : stream(st) {
+    if (!g_prof_on.load(std::memory_order_relaxed)) return;
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    if (g_prof_used + 2 > g_prof_pool.size()) return;
+    ProfileRecord r{name, g_prof_pool[g_prof_used], g_prof_pool[g_prof_used + 1]};
+    g_prof_used += 2;
+    if (cudaEventRecord(r.start, st) != cudaSuccess) return;
+    g_prof_pending.push_back(r);
+    index = long(g_prof_pending.size()) - 1;
+}
+
+ProfileScope::~ProfileScope() {
+    if (index < 0) return;
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    if (size_t(index) < g_prof_pending.size()) cudaEventRecord(g_prof_pending[index].stop, stream);
+}
+
+int profile_enable(uint32_t capacity) {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    g_prof_on = false;
+    for (auto& r : g_prof_pending) {
+        cudaEventSynchronize(r.stop);
+    }
+    for (auto e : g_prof_pool) cudaEventDestroy(e);
+    g_prof_pool.clear();
+    g_prof_pending.clear();
+    g_prof_totals.clear();
+    g_prof_used = 0;
+    if (!capacity) return PM_OK;
+    g_prof_pool.resize(2 * size_t(capacity));
+    for (auto& e : g_prof_pool)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            g_prof_pool.clear();
+            return fail(PM_ERR_CUDA, "cannot create profiling events");
+        }
+    g_prof_on = true;
+    return PM_OK;
+}
+
+int profile_read(const char** names, uint64_t* launches, double* total_ms, uint32_t capacity, uint32_t* count) {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    for (auto& r : g_prof_pending) {
+        float ms = 0;
+        if (cudaEventSynchronize(r.stop) != cudaSuccess || cudaEventElapsedTime(&ms, r.start, r.stop) != cudaSuccess)
+            return fail(PM_ERR_CUDA, "profiling event failed");
+        bool found = false;
+        for (auto& t : g_prof_totals)
+            if (t.name == r.name) {
+                ++t.launches;
+                t.ms += ms;
+                found = true;
+            }
+        if (!found) g_prof_totals.push_back({r.name, 1, ms});
+    }
+    g_prof_pending.clear();
+    g_prof_used = 0;
+    *count = uint32_t(g_prof_totals.size());
+    for (uint32_t i = 0; i < capacity && i < g_prof_totals.size(); ++i) {
+        names[i] = g_prof_totals[i].name;
+        launches[i] = g_prof_totals[i].launches;
+        total_ms[i] = g_prof_totals[i].ms;
+    }
+    return PM_OK;
+}
+
+int fail(int status, const std::string& message) {
+    g_last_error = message;
+    return status;
+}
+
+// ---------------------------------------------------------------------------
+// The prime basis: primes p = 1 mod 2^17 below 2^30, descending, with
+// psi-merged bit-reversed twiddle tables of length 65536 per prime.  The table
+// of a smaller ring n is the length-n prefix of the same table, so one copy
+// per device serves every plan (the reference builds per-n tables,
+// rns/host_setup.h:108-124).
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_basis_mutex;
+std::vector<std::unique_ptr<DeviceBasis>> g_basis;  // index = device ordinal
+}  // namespace
+
+std::vector<uint32_t> make_primes() {
+    std::vector<uint32_t> primes;
+    const uint32_t order = 1u << (kLogNMax + 1);
+    for (uint64_t cand = (uint64_t(1) << 30) - order + 1; primes.size() < unsigned(kPMax); cand -= order) {
+        if (cand <= (uint64_t(1) << 29)) throw Failure(PM_ERR_UNSUPPORTED, "prime search ran below 2^29");
+        if (is_prime32(uint32_t(cand))) primes.push_back(uint32_t(cand));
+    }
+    return primes;
+}
+
+namespace {
+// psi of multiplicative order exactly 2 * 65536
+uint32_t root_of_unity(uint32_t p) {
+    const uint64_t order = uint64_t(2) << kLogNMax;
+    for (uint32_t g = 2; g < 1000000; ++g) {
+        const uint32_t root = powmod(g, (p - 1) / order, p);
+        if (powmod(root, order / 2, p) == p - 1) return root;
+    }
+    throw Failure(PM_ERR_UNSUPPORTED, "no root of unity of order 2^17");
+}
+}  // namespace
+
+DeviceBasis::~DeviceBasis() {
+    cudaSetDevice(device);
+    cudaFree(d_pc);
+    cudaFree(d_tw_fwd);
+    cudaFree(d_tw_inv);
+    cudaFree(d_conv_pow);
+}
+
+DeviceBasis& basis_for_device(int device) {
+    std::lock_guard<std::mutex> lock(g_basis_mutex);
+    if (device < 0) throw Failure(PM_ERR_INVALID, "bad device ordinal");
+    if (g_basis.size() <= size_t(device)) g_basis.resize(device + 1);
+    if (g_basis[device]) return *g_basis[device];
+    auto B = std::make_unique<DeviceBasis>();
+    B->device = device;
+    B->primes = make_primes();
+    const size_t P = B->primes.size();
+    std::vector<PrimeConst> pc(P);
+    std::vector<uint2> fwd(P * kNMax), inv(P * kNMax), pow(P * kPowWords);
+    auto fill = [&](size_t begin, size_t end) {
+        std::vector<uint32_t> ppow(kNMax), ipow(kNMax);
+        for (size_t i = begin; i < end; ++i) {
+            const uint32_t p = B->primes[i];
+            const uint32_t psi = root_of_unity(p), ipsi = powmod(psi, p - 2, p);
+            ppow[0] = ipow[0] = 1;
+            for (int e = 1; e < kNMax; ++e) {
+                ppow[e] = mulmod(ppow[e - 1], psi, p);
+                ipow[e] = mulmod(ipow[e - 1], ipsi, p);
+            }
+            for (int k = 0; k < kNMax; ++k) {
+                const uint32_t e = bit_reverse(uint32_t(k), kLogNMax);
+                fwd[i * kNMax + k] = make_uint2(ppow[e], shoup_of(ppow[e], p));
+                inv[i * kNMax + k] = make_uint2(ipow[e], shoup_of(ipow[e], p));
+            }
+            uint32_t w = 1;
+            const uint32_t base = uint32_t((uint64_t(1) << 32) % p);
+            for (int k = 0; k < kPowWords; ++k) {
+                pow[i * kPowWords + k] = make_uint2(w, shoup_of(w, p));
+                w = mulmod(w, base, p);
+            }
+            pc[i].p = p;
+            pc[i].two_p = 2 * p;
+            pc[i].mu = uint32_t((uint64_t(1) << 61) / p);
+            pc[i].pad = 0;
+            pc[i].recip = uint64_t(((unsigned __int128)1 << 64) / p);
+        }
+    };
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt == 0 ? 1 : (nt > 16 ? 16 : nt);
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t) pool.emplace_back(fill, P * t / nt, P * (t + 1) / nt);
+    for (auto& th : pool) th.join();
+
+    int previous = 0;
+    cuda_check(cudaGetDevice(&previous), "cudaGetDevice");
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cuda_check(cudaMalloc(&B->d_pc, P * sizeof(PrimeConst)), "allocate prime constants");
+    cuda_check(cudaMalloc(&B->d_tw_fwd, fwd.size() * sizeof(uint2)), "allocate forward twiddles");
+    cuda_check(cudaMalloc(&B->d_tw_inv, inv.size() * sizeof(uint2)), "allocate inverse twiddles");
+    cuda_check(cudaMalloc(&B->d_conv_pow, pow.size() * sizeof(uint2)), "allocate limb powers");
+    cuda_check(cudaMemcpy(B->d_pc, pc.data(), P * sizeof(PrimeConst), cudaMemcpyHostToDevice), "upload primes");
+    cuda_check(cudaMemcpy(B->d_tw_fwd, fwd.data(), fwd.size() * sizeof(uint2), cudaMemcpyHostToDevice),
+               "upload forward twiddles");
+    cuda_check(cudaMemcpy(B->d_tw_inv, inv.data(), inv.size() * sizeof(uint2), cudaMemcpyHostToDevice),
+               "upload inverse twiddles");
+    cuda_check(cudaMemcpy(B->d_conv_pow, pow.data(), pow.size() * sizeof(uint2), cudaMemcpyHostToDevice),
+               "upload limb powers");
+    cuda_check(cudaSetDevice(previous), "cudaSetDevice");
+    g_basis[device] = std::move(B);
+    return *g_basis[device];
+}
+
+// Smallest prefix of the basis with product above 2^(2*bits(q) + 2 + log2 n):
+// the negacyclic coefficients lie in (-n(q-1)^2, n(q-1)^2), and a quarter of
+// the CRT range is what the nearest-quotient correction needs
+// (rns/host_setup.h:81-83 checks P > 4N(q-1)^2 the same way).
+unsigned basis_size(const std::vector<uint32_t>& primes, unsigned n, unsigned qbits) {
+    unsigned logn = 0;
+    while ((1u << logn) < n) ++logn;
+    const unsigned need = 2 * qbits + 2 + logn + 1;  // bit_length(P) >= need  <=>  P > 2^(need-1)
+    Words P{1};
+    for (unsigned i = 0; i < primes.size(); ++i) {
+        P = multiply_small(P, primes[i]);
+        if (bit_length(P) >= need) return i + 1;
+    }
+    throw Failure(PM_ERR_UNSUPPORTED, "q too wide for the prime basis");
+}
+
+// ---------------------------------------------------------------------------
+// plans
+// ---------------------------------------------------------------------------
+PlanCore::~PlanCore() {
+    int previous = 0;
+    cudaGetDevice(&previous);
+    cudaSetDevice(device);
+    cudaFree(d_mq);
+    cudaFree(d_consts);
+    cudaFree(d_scale);
+    cudaFree(d_work);
+    cudaFree(d_io);
+    cudaFreeHost(h_stage);
+    if (stream) cudaStreamDestroy(stream);
+    cudaSetDevice(previous);
+}
+
+void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs_, uint32_t flags_) {
+    if (!q64 || q_limbs == 0) throw Failure(PM_ERR_INVALID, "q is missing");
+    if (n_ < 2 || (n_ & (n_ - 1))) throw Failure(PM_ERR_INVALID, "n must be a power of two >= 2");
+    if (n_ > uint32_t(kNMax)) throw Failure(PM_ERR_UNSUPPORTED, "n above 65536");
+    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR)) throw Failure(PM_ERR_INVALID, "unknown flags");
+    q.assign(2 * q_limbs, 0);
+    for (uint32_t i = 0; i < q_limbs; ++i) {
+        q[2 * i] = uint32_t(q64[i]);
+        q[2 * i + 1] = uint32_t(q64[i] >> 32);
+    }
+    trim(q);
+    qbits = bit_length(q);
+    if (qbits < 2 || !(q[0] & 1)) throw Failure(PM_ERR_INVALID, "q must be odd and at least 3");
+    if (qbits > 32u * kWMax) throw Failure(PM_ERR_UNSUPPORTED, "q wider than 896 bits");
+    const uint32_t qwords = (qbits + 31) / 32;
+    if (uint64_t(coef_limbs_) * 64 < qbits) throw Failure(PM_ERR_INVALID, "coef_limbs too small for q");
+    if (coef_limbs_ > 64) throw Failure(PM_ERR_UNSUPPORTED, "coef_limbs above 64");
+    n = n_;
+    logn = 0;
+    while ((1u << logn) < n) ++logn;
+    logR = logn < 5 ? logn : 5;
+    logC = logn - logR;
+    coef_limbs = coef_limbs_;
+    stride = 2 * coef_limbs;
+    W = (qwords + 3) / 4 * 4;
+    if (W < 4) W = 4;
+    flags = flags_;
+    cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+    basis = &basis_for_device(device);
+    P = basis_size(basis->primes, n, qbits);
+
+    // CRT constants: (P_total / p_i) mod q, (-P_total) mod q, scale = n^-1 (P/p_i)^-1 mod p_i
+    Words total{1};
+    for (unsigned i = 0; i < P; ++i) total = multiply_small(total, basis->primes[i]);
+    std::vector<uint32_t> mq(size_t(P) * W, 0), consts(2 * size_t(W), 0);
+    std::vector<uint2> scale(P);
+    for (unsigned i = 0; i < P; ++i) {
+        const uint32_t p = basis->primes[i];
+        Words m = total;
+        if (divide_small(m, p)) throw Failure(PM_ERR_UNSUPPORTED, "basis product not divisible");
+        const Words mmod = padded(mod(m, q), W);
+        std::copy(mmod.begin(), mmod.end(), mq.begin() + size_t(i) * W);
+        const uint32_t minv = powmod(mod_small(m, p), p - 2, p);
+        const uint32_t ninv = powmod(n % p, p - 2, p);
+        const uint32_t s = mulmod(minv, ninv, p);
+        scale[i] = make_uint2(s, shoup_of(s, p));
+    }
+    const Words qpad = padded(q, W);
+    Words pmod = mod(total, q);
+    const Words pneg = padded(compare(pmod, Words{}) == 0 ? Words{} : subtract(q, pmod), W);
+    std::copy(qpad.begin(), qpad.end(), consts.begin());
+    std::copy(pneg.begin(), pneg.end(), consts.begin() + W);
+    // mu_q = floor(2^(qbits + 62) / q)
+    Words quo;
+    Words num(((qbits + 62) / 32) + 1, 0);
+    num[(qbits + 62) / 32] = 1u << ((qbits + 62) % 32);
+    divmod(num, q, &quo, nullptr);
+    quo.resize(2, 0);
+    mu_q = (uint64_t(quo[1]) << 32) | quo[0];
+
+    workspace_bytes = size_t(2) * P * n * sizeof(uint32_t);
+    io_bytes = size_t(n) * coef_limbs * sizeof(uint64_t);
+    cuda_check(cudaMalloc(&d_mq, mq.size() * 4), "allocate CRT rows");
+    cuda_check(cudaMalloc(&d_consts, consts.size() * 4), "allocate q constants");
+    cuda_check(cudaMalloc(&d_scale, scale.size() * sizeof(uint2)), "allocate CRT scales");
+    cuda_check(cudaMemcpy(d_mq, mq.data(), mq.size() * 4, cudaMemcpyHostToDevice), "upload CRT rows");
+    cuda_check(cudaMemcpy(d_consts, consts.data(), consts.size() * 4, cudaMemcpyHostToDevice), "upload q");
+    cuda_check(cudaMemcpy(d_scale, scale.data(), scale.size() * sizeof(uint2), cudaMemcpyHostToDevice),
+               "upload CRT scales");
+    cuda_check(cudaMalloc(&d_work, workspace_bytes), "allocate residue workspace");
+    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "create plan stream");
+    if (flags & PM_CONVERT_TENSOR) tensor_init(*this);
+}
+
+// ---------------------------------------------------------------------------
+// launch sequence of one product: K1 -> K2 -> K3 on one stream
+// ---------------------------------------------------------------------------
+namespace {
+template <int W>
+void launch_k1(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, cudaStream_t st) {
+    const int G = s.logC >= 3 ? 8 : (1 << s.logC);
+    dim3 grid((1u << s.logC) / G, 2), block((1u << s.logR) * G);
+    k1_convert_cols<W><<<grid, block, 0, st>>>(a, b, work, s.basis->d_pc, s.basis->d_conv_pow, s.basis->d_tw_fwd,
+                                                int(s.n), int(s.logR), int(s.logC), int(s.P), int(s.stride));
+}
+
+template <int W>
+void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, cudaStream_t st) {
+    const int G = s.logC >= 3 ? 8 : (1 << s.logC);
+    dim3 grid((1u << s.logC) / G), block((1u << s.logR) * G);
+    const size_t smem = size_t(s.P) * W * 4;
+    k3_cols_crt<W><<<grid, block, smem, st>>>(work, c, s.basis->d_pc, s.basis->d_tw_inv, s.d_scale, s.d_mq,
+                                              s.d_consts, s.mu_q, int(s.qbits), int(s.n), int(s.logR),
+                                              int(s.logC), int(s.P), int(s.stride));
+}
+
+template <int LOGC>
+void launch_k2_fixed(const PlanCore& s, uint32_t* work, cudaStream_t st) {
+    constexpr int C = 1 << LOGC, T = C / 8;
+    int rows = T >= 128 ? 1 : 128 / T;
+    const int R = 1 << s.logR;
+    if (rows > R) rows = R;
+    const size_t smem = size_t(rows) * 2 * C * 4;
+    if (smem > 48 * 1024)
+        cuda_check(cudaFuncSetAttribute(k2_rows<LOGC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                   "raise K2 shared memory");
+    dim3 grid(R / rows, s.P), block(rows * T);
+    k2_rows<LOGC><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.n),
+                                             int(s.logR), int(s.P));
+}
+
+void launch_k2(const PlanCore& s, uint32_t* work, cudaStream_t st) {
+    switch (s.logC) {
+        case 3: return launch_k2_fixed<3>(s, work, st);
+        case 4: return launch_k2_fixed<4>(s, work, st);
+        case 5: return launch_k2_fixed<5>(s, work, st);
+        case 6: return launch_k2_fixed<6>(s, work, st);
+        case 7: return launch_k2_fixed<7>(s, work, st);
+        case 8: return launch_k2_fixed<8>(s, work, st);
+        case 9: return launch_k2_fixed<9>(s, work, st);
+        case 10: return launch_k2_fixed<10>(s, work, st);
+        case 11: return launch_k2_fixed<11>(s, work, st);
+        default: {
+            const int R = 1 << s.logR;
+            dim3 grid((R + 31) / 32, s.P), block(R < 32 ? R : 32);
+            k2_rows_small<<<grid, block, 0, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
+                                                 int(s.n), int(s.logR), int(s.logC), int(s.P));
+        }
+    }
+}
+
+#define PM_DISPATCH_W(W_, CALL)                                          \
+    switch (W_) {                                                       \
+        case 4: CALL(4); break;                                         \
+        case 8: CALL(8); break;                                         \
+        case 12: CALL(12); break;                                       \
+        case 16: CALL(16); break;                                       \
+        case 20: CALL(20); break;                                       \
+        case 24: CALL(24); break;                                       \
+        case 28: CALL(28); break;                                       \
+        default: throw Failure(PM_ERR_UNSUPPORTED, "unsupported width"); \
+    }
+}  // namespace
+
+void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
+                 cudaStream_t st) {
+    {
+        ProfileScope prof("k1_convert_cols", st);
+#define PM_K1(W) launch_k1<W>(s, a, b, work, st)
+        PM_DISPATCH_W(s.W, PM_K1)
+#undef PM_K1
+    }
+    {
+        ProfileScope prof("k2_rows", st);
+        launch_k2(s, work, st);
+    }
+    {
+        ProfileScope prof("k3_cols_crt", st);
+#define PM_K3(W) launch_k3<W>(s, work, c, st)
+        PM_DISPATCH_W(s.W, PM_K3)
+#undef PM_K3
+    }
+    cuda_check(cudaGetLastError(), "launch product kernels");
+    count_launches(3);
+}
+
+void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
+                    cudaStream_t st) {
+    uint32_t* work = workspace ? static_cast<uint32_t*>(workspace) : s.d_work;
+    const uint32_t* a32 = reinterpret_cast<const uint32_t*>(a);
+    const uint32_t* b32 = reinterpret_cast<const uint32_t*>(b);
+    uint32_t* c32 = reinterpret_cast<uint32_t*>(c);
+    if (s.flags & PM_CONVERT_TENSOR)
+        launch_tensor(s, a32, b32, c32, work, st);
+    else
+        launch_simt(s, a32, b32, c32, work, st);
+}
+
+// Host buffers: pinned memory is copied directly; pageable memory is staged
+// through the plan's pinned buffer (one memcpy each way).
+void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c) {
+    if (!s.d_io) {
+        cuda_check(cudaMalloc(&s.d_io, 3 * s.io_bytes), "allocate plan I/O buffers");
+        cuda_check(cudaMallocHost(&s.h_stage, 3 * s.io_bytes), "allocate pinned staging");
+    }
+    auto pinned = [](const void* p) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    uint8_t* dev = static_cast<uint8_t*>(s.d_io);
+    uint8_t* stage = static_cast<uint8_t*>(s.h_stage);
+    const bool pa = pinned(a), pb = pinned(b), pc = pinned(c);
+    const void* src_a = a;
+    const void* src_b = b;
+    if (!pa) {
+        std::memcpy(stage, a, s.io_bytes);
+        src_a = stage;
+    }
+    if (!pb) {
+        std::memcpy(stage + s.io_bytes, b, s.io_bytes);
+        src_b = stage + s.io_bytes;
+    }
+    cuda_check(cudaMemcpyAsync(dev, src_a, s.io_bytes, cudaMemcpyHostToDevice, s.stream), "copy a to device");
+    cuda_check(cudaMemcpyAsync(dev + s.io_bytes, src_b, s.io_bytes, cudaMemcpyHostToDevice, s.stream),
+               "copy b to device");
+    launch_product(s, reinterpret_cast<const uint64_t*>(dev), reinterpret_cast<const uint64_t*>(dev + s.io_bytes),
+                   reinterpret_cast<uint64_t*>(dev + 2 * s.io_bytes), nullptr, s.stream);
+    void* dst = pc ? static_cast<void*>(c) : static_cast<void*>(stage + 2 * s.io_bytes);
+    cuda_check(cudaMemcpyAsync(dst, dev + 2 * s.io_bytes, s.io_bytes, cudaMemcpyDeviceToHost, s.stream),
+               "copy c to host");
+    cuda_check(cudaStreamSynchronize(s.stream), "product");
+    if (!pc) std::memcpy(c, stage + 2 * s.io_bytes, s.io_bytes);
+}
+
+}  // namespace pm
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct pm_plan {
+    pm::PlanCore core;
+};
+
+using pm::fail;
+using pm::Failure;
+
+#define PM_GUARD(body)                                                   \
+    try {                                                                \
+        body;                                                            \
+        return PM_OK;                                                    \
+    } catch (const Failure& f) {                                         \
+        return fail(f.status, f.what());                                 \
+    } catch (const std::bad_alloc&) {                                    \
+        return fail(PM_ERR_NO_MEMORY, "host allocation failed");         \
+    } catch (const std::exception& e) {                                  \
+        return fail(PM_ERR_INVALID, e.what());                           \
+    }
+
+extern "C" int pm_plan_create(pm_plan** plan, uint32_t n, const uint64_t* q, uint32_t q_limbs, uint32_t coef_limbs,
+                              uint32_t flags) {
+    if (!plan) return fail(PM_ERR_INVALID, "plan pointer is NULL");
+    *plan = nullptr;
+    PM_GUARD({
+        auto p = std::make_unique<pm_plan>();
+        p->core.init(n, q, q_limbs, coef_limbs, flags);
+        *plan = p.release();
+    })
+}
+
+extern "C" int pm_plan_get_info(const pm_plan* plan, pm_plan_info* info) {
+    if (!plan || !info) return fail(PM_ERR_INVALID, "NULL argument");
+    const auto& s = plan->core;
+    info->n = s.n;
+    info->q_bits = s.qbits;
+    info->coef_limbs = s.coef_limbs;
+    info->primes = s.P;
+    info->convert = s.flags & PM_CONVERT_TENSOR;
+    info->reserved = 0;
+    info->workspace_bytes = s.workspace_bytes;
+    return PM_OK;
+}
+
+extern "C" int pm_plan_destroy(pm_plan* plan) {
+    if (!plan) return PM_OK;
+    PM_GUARD({
+        cudaStreamSynchronize(plan->core.stream);
+        delete plan;
+    })
+}
+
+extern "C" int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
+                           pm_stream stream) {
+    if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
+    PM_GUARD(pm::launch_product(plan->core, a, b, c, workspace, reinterpret_cast<cudaStream_t>(stream)))
+}
+
+extern "C" int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c) {
+    if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
+    PM_GUARD(pm::multiply_host(plan->core, a, b, c))
+}
+
+extern "C" int pm_basis_query(uint32_t n, uint32_t q_bits, uint32_t* primes, uint32_t capacity, uint32_t* count) {
+    if (!count) return fail(PM_ERR_INVALID, "count pointer is NULL");
+    *count = 0;
+    if (n < 2 || (n & (n - 1))) return fail(PM_ERR_INVALID, "n must be a power of two >= 2");
+    if (n > uint32_t(pm::kNMax)) return fail(PM_ERR_UNSUPPORTED, "n above 65536");
+    if (q_bits < 2 || q_bits > 32u * pm::kWMax) return fail(PM_ERR_UNSUPPORTED, "q_bits outside [2, 896]");
+    PM_GUARD({
+        static const std::vector<uint32_t> all = pm::make_primes();
+        const unsigned k = pm::basis_size(all, n, q_bits);
+        *count = k;
+        for (unsigned i = 0; i < k && i < capacity; ++i) primes[i] = all[i];
+    })
+}
+
+extern "C" const char* pm_status_string(int status) {
+    switch (status) {
+        case PM_OK: return "ok";
+        case PM_ERR_INVALID: return "invalid argument";
+        case PM_ERR_UNSUPPORTED: return "unsupported parameters";
+        case PM_ERR_CUDA: return "CUDA error";
+        case PM_ERR_NO_MEMORY: return "out of memory";
+        case PM_ERR_TIMEOUT: return "timed out";
+        case PM_ERR_BUSY: return "busy";
+        default: return "unknown status";
+    }
+}
+
+extern "C" const char* pm_last_error(void) { return pm::g_last_error.c_str(); }
+
+extern "C" uint64_t pm_kernel_launch_count(void) { return pm::g_launches.load(); }
+
+extern "C" int pm_profile_enable(uint32_t capacity) { return pm::profile_enable(capacity); }
+
+extern "C" int pm_profile_read(const char** names, uint64_t* launches, double* total_ms, uint32_t capacity,
+                               uint32_t* count) {
+    if (!count || (capacity && (!names || !launches || !total_ms))) return fail(PM_ERR_INVALID, "NULL argument");
+    return pm::profile_read(names, launches, total_ms, capacity, count);
+}

@@ -1,0 +1,164 @@
+"""Python binding of libpolymul (include/polymul.h) over ctypes.
+
+Host-side mirror of the reference's solution interface for the tests and the
+benchmark: ``Plan`` plays fherma_init / fherma_free (fherma.h:44,46) and
+``Plan.multiply_host`` plays fherma_run (fherma.h:45) on (n, limbs) uint64
+coefficient arrays.  Errors raise ``PolymulError`` carrying the library's
+status code and message, the way the reference raises std::runtime_error
+(rns/solve.cu:421-423).
+
+The library must be built (``make -C fherma-polymul-baseline_b200``); there is
+no fallback -- a missing library is an ImportError-class failure.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpolymul.so")
+
+PM_OK = 0
+PM_ERR_INVALID = 1
+PM_ERR_UNSUPPORTED = 2
+PM_ERR_CUDA = 3
+PM_ERR_NO_MEMORY = 4
+PM_ERR_TIMEOUT = 5
+PM_ERR_BUSY = 6
+PM_CONVERT_SIMT = 0
+PM_CONVERT_TENSOR = 1
+
+_lib = None
+
+
+class PolymulError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("q_bits", ctypes.c_uint32), ("coef_limbs", ctypes.c_uint32),
+                ("primes", ctypes.c_uint32), ("convert", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("workspace_bytes", ctypes.c_size_t)]
+
+
+def lib():
+    """Load libpolymul.so once; raises OSError when it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with make -C {HERE}")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, u64p = ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)
+        L.pm_plan_create.argtypes = [ctypes.POINTER(vp), u32, u64p, u32, u32, u32]
+        L.pm_plan_get_info.argtypes = [vp, ctypes.POINTER(PlanInfo)]
+        L.pm_plan_destroy.argtypes = [vp]
+        L.pm_multiply.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.pm_multiply_host.argtypes = [vp, vp, vp, vp]
+        L.pm_basis_query.argtypes = [u32, u32, ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
+        L.pm_status_string.restype = ctypes.c_char_p
+        L.pm_status_string.argtypes = [ctypes.c_int]
+        L.pm_last_error.restype = ctypes.c_char_p
+        L.pm_kernel_launch_count.restype = ctypes.c_uint64
+        L.pm_profile_enable.argtypes = [ctypes.c_uint32]
+        L.pm_profile_read.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint64),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.c_uint32, ctypes.POINTER(u32)]
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != PM_OK:
+        raise PolymulError(status, lib().pm_last_error().decode(errors="replace"))
+
+
+def q_limbs_of(q):
+    q = int(q)
+    limbs = max(1, (q.bit_length() + 63) // 64)
+    return np.frombuffer(q.to_bytes(8 * limbs, "little"), dtype=np.uint64).copy()
+
+
+def basis(n, q_bits):
+    """Primes of the RNS basis for (n, q_bits); needs no GPU."""
+    buf = (ctypes.c_uint32 * 128)()
+    count = ctypes.c_uint32(0)
+    check(lib().pm_basis_query(n, q_bits, buf, 128, ctypes.byref(count)))
+    return [buf[i] for i in range(count.value)]
+
+
+def launch_count():
+    return int(lib().pm_kernel_launch_count())
+
+
+def profile_enable(capacity):
+    """Record device time of each library kernel launch (up to `capacity` launches)."""
+    check(lib().pm_profile_enable(capacity))
+
+
+def profile_read():
+    """{kernel name: (launches, total device ms)} since profile_enable."""
+    cap = 64
+    names = (ctypes.c_char_p * cap)()
+    launches = (ctypes.c_uint64 * cap)()
+    ms = (ctypes.c_double * cap)()
+    count = ctypes.c_uint32(0)
+    check(lib().pm_profile_read(names, launches, ms, cap, ctypes.byref(count)))
+    return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(min(cap, count.value))}
+
+
+class Plan:
+    """A product plan for (n, q): basis, CRT constants, workspace, staging."""
+
+    def __init__(self, n, q, coef_limbs=None, tensor=False):
+        self.q = int(q)
+        qarr = q_limbs_of(self.q)
+        self.n = int(n)
+        self.coef_limbs = int(coef_limbs) if coef_limbs else len(qarr)
+        self._h = ctypes.c_void_p()
+        check(lib().pm_plan_create(ctypes.byref(self._h), self.n,
+                                   qarr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(qarr),
+                                   self.coef_limbs, PM_CONVERT_TENSOR if tensor else PM_CONVERT_SIMT))
+        info = PlanInfo()
+        check(lib().pm_plan_get_info(self._h, ctypes.byref(info)))
+        self.info = info
+        self.primes = info.primes
+        self.workspace_bytes = info.workspace_bytes
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().pm_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _shape_ok(self, x):
+        x = np.ascontiguousarray(x, dtype=np.uint64)
+        if x.shape != (self.n, self.coef_limbs):
+            raise PolymulError(PM_ERR_INVALID, f"expected shape {(self.n, self.coef_limbs)}, got {x.shape}")
+        return x
+
+    def multiply_host(self, a, b, out=None):
+        """c = a*b mod (X^n+1, q) for host arrays; synchronous."""
+        a, b = self._shape_ok(a), self._shape_ok(b)
+        c = np.empty_like(a) if out is None else out
+        check(lib().pm_multiply_host(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
+        return c
+
+    def multiply(self, a_ptr, b_ptr, c_ptr, workspace=0, stream=0):
+        """Asynchronous product on device pointers (ints) on a CUDA stream handle."""
+        check(lib().pm_multiply(self._h, a_ptr, b_ptr, c_ptr, workspace or None, stream or None))

@@ -1,0 +1,120 @@
+/*
+ * polymul.h -- C ABI of the B200 exact negacyclic multiplier
+ *
+ *     c = a * b  mod (X^n + 1, q)     n a power of two, 2 <= n <= 65536,
+ *                                      q odd, up to 896 bits.
+ *
+ * Coefficients are little-endian 64-bit limbs, `coef_limbs` per coefficient,
+ * row-major n x coef_limbs, each value in [0, q).  For the reference's point
+ * (N x 28 x u32, fherma.h:27-42) that is n x 14 u64 -- the same bytes.
+ *
+ * Every entry point returns a pm_status; on failure pm_last_error() gives a
+ * message for the calling thread.  No entry point throws, and none takes or
+ * returns a framework type: plain pointers, sizes and a CUDA stream handle.
+ *
+ * The reference's drop-in boundary is three C++ functions (fherma.h:44-46);
+ * fherma_polymul.h declares those, implemented on top of this header.
+ */
+#ifndef POLYMUL_H
+#define POLYMUL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pm_plan pm_plan;
+/* A cudaStream_t; NULL means the legacy default stream. */
+typedef struct CUstream_st* pm_stream;
+
+enum pm_status {
+    PM_OK = 0,
+    PM_ERR_INVALID = 1,     /* bad argument: n not a power of two, even q, short buffers, ... */
+    PM_ERR_UNSUPPORTED = 2, /* outside coverage: n > 65536, q wider than 896 bits, ... */
+    PM_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    PM_ERR_NO_MEMORY = 4,   /* device or pinned host allocation failed */
+    PM_ERR_TIMEOUT = 5,     /* a bounded wait ran out */
+    PM_ERR_BUSY = 6         /* admission refused: no slot or device memory free */
+};
+
+/* Residue conversion and CRT implementation. */
+enum pm_flags {
+    PM_CONVERT_SIMT = 0,   /* scalar CUDA-core conversion and CRT (the plain method) */
+    PM_CONVERT_TENSOR = 1  /* exact INT8 digit contractions on the tcgen05 tensor cores */
+};
+
+typedef struct {
+    uint32_t n;
+    uint32_t q_bits;
+    uint32_t coef_limbs;
+    uint32_t primes;          /* RNS basis size for (n, q) */
+    uint32_t convert;         /* PM_CONVERT_* the plan runs */
+    uint32_t reserved;
+    size_t workspace_bytes;   /* device scratch one product needs (residue planes) */
+} pm_plan_info;
+
+/*
+ * Build a plan: choose the prime basis, upload CRT constants, allocate the
+ * plan's own device workspace and pinned staging.  Untimed set-up.
+ * Replaces fherma_init (fherma.h:44; rns/solve.cu:581-720, rns/host_setup.h:61-126),
+ * widened from q = 2^868 - c to any odd q and from n <= 32768 to n <= 65536.
+ * q: q_limbs little-endian u64 words.  coef_limbs >= ceil(bits(q) / 64).
+ */
+int pm_plan_create(pm_plan** plan, uint32_t n, const uint64_t* q, uint32_t q_limbs, uint32_t coef_limbs,
+                   uint32_t flags);
+
+int pm_plan_get_info(const pm_plan* plan, pm_plan_info* info);
+
+/* Replaces fherma_free (fherma.h:46; rns/solve.cu:854). */
+int pm_plan_destroy(pm_plan* plan);
+
+/*
+ * One product on device memory, asynchronous on `stream`.  a, b, c are device
+ * pointers (n x coef_limbs u64); c may alias neither a nor b.  workspace is a
+ * device buffer of info.workspace_bytes, or NULL to use the plan's own (then
+ * calls on one plan must not overlap).  Replaces the device half of fherma_run
+ * (rns/solve.cu:504-578, launch_rns).
+ */
+int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
+                pm_stream stream);
+
+/*
+ * One product on host memory, synchronous: copy in, multiply, copy out.
+ * Pinned (page-locked) buffers are copied directly; pageable ones are staged
+ * through the plan's pinned buffers.  Replaces fherma_run (fherma.h:45;
+ * rns/solve.cu:721-853).
+ */
+int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c);
+
+/*
+ * Host-only (no GPU needed): the RNS basis a plan for (n, q_bits) would use.
+ * Writes up to `capacity` primes (descending, p = 1 mod 2^17, p < 2^30) and
+ * sets *count.  Mirrors rns::setup's prime search (rns/host_setup.h:67-83).
+ */
+int pm_basis_query(uint32_t n, uint32_t q_bits, uint32_t* primes, uint32_t capacity, uint32_t* count);
+
+const char* pm_status_string(int status);
+/* Message of the last failure on the calling thread ("" if none). */
+const char* pm_last_error(void);
+/* Number of kernel launches the library issued on this process so far. */
+uint64_t pm_kernel_launch_count(void);
+
+/*
+ * Kernel timing for measurement runs.  pm_profile_enable(capacity) makes the
+ * library record a CUDA event before and after each kernel it launches, on the
+ * launching stream, for up to `capacity` launches (0 switches it off and drops
+ * pending records).  pm_profile_read synchronizes those events and returns,
+ * per kernel name, the launch count and summed device milliseconds; names stay
+ * valid for the life of the process.  Plays the role of the reference's
+ * FHERMA_PROFILE stage events (rns/solve.cu:474-486, 819-835).
+ */
+int pm_profile_enable(uint32_t capacity);
+int pm_profile_read(const char** names, uint64_t* launches, double* total_ms, uint32_t capacity, uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLYMUL_H */

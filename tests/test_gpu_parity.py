@@ -1,0 +1,110 @@
+"""GPU parity of the plain (SIMT conversion/CRT) path through the C ABI.
+
+Bit-exact: every product must equal the oracle's canonical residue in [0, q).
+The reference's golden points (tests/golden/golden.json, produced by its own
+tests/validate.py) are checked by SHA-256; other sizes and widths against the
+C oracle on the same seeded inputs.
+"""
+import numpy as np
+import pytest
+
+import polymul
+from oracle import oracle
+from tests.golden.cases import point_cases, sha
+from tests.helpers import random_q, uniform_below
+
+pytestmark = pytest.mark.gpu
+
+TENSOR = False
+
+
+def plan(n, q, limbs=None):
+    return polymul.Plan(n, q, coef_limbs=limbs, tensor=TENSOR)
+
+
+def test_golden_points(cuda, golden):
+    for point in golden["points"]:
+        q = int(point["q"], 16)
+        with plan(point["N"], q, 14) as p:
+            for label, a, b, rec in point_cases(point):  # same plan reused across cases
+                c = p.multiply_host(a, b)
+                assert sha(c.tobytes()) == rec["c_sha256"], (point["N"], point["delta"], label)
+
+
+@pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 64, 128, 256, 512, 2048, 8192, 16384, 65536])
+def test_ring_sizes_868(cuda, n):
+    rng = np.random.default_rng(n)
+    q = random_q(rng, 868)
+    a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
+    with plan(n, q, 14) as p:
+        assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
+
+
+@pytest.mark.parametrize("bits", [3, 31, 64, 65, 129, 200, 257, 384, 517, 640, 700, 800, 867, 896])
+def test_widths(cuda, bits):
+    n = 1024
+    rng = np.random.default_rng(bits)
+    q = random_q(rng, bits)
+    a, b = uniform_below(rng, q, n), uniform_below(rng, q, n)
+    with plan(n, q) as p:
+        assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
+
+
+def test_padded_limbs(cuda):
+    """Coefficients stored wider than q needs (the fherma layout keeps 28 words for any q)."""
+    rng = np.random.default_rng(3)
+    q = random_q(rng, 200)
+    a, b = uniform_below(rng, q, 256, 14), uniform_below(rng, q, 256, 14)
+    with plan(256, q, 14) as p:
+        c = p.multiply_host(a, b)
+    assert (c == oracle.rns_multiply(a, b, q)).all()
+    assert not c[:, 4:].any()
+
+
+def test_edge_values_full_size(cuda):
+    n = 32768
+    q = (1 << 868) - 1  # not prime: any odd q is accepted
+    vals = [0, 1, q - 1, q - 2, 1 << 864, (1 << 864) - 1, 1 << 32, (1 << 32) - 1, (1 << 867), 2]
+    rng = np.random.default_rng(11)
+    idx = rng.integers(0, len(vals), size=n)
+    from tests.helpers import from_ints
+    a = from_ints([vals[i] for i in idx], 14)
+    b = from_ints([vals[i] for i in rng.permutation(idx)], 14)
+    with plan(n, q, 14) as p:
+        assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
+
+
+def test_device_pointers_and_external_workspace(cuda):
+    torch = cuda
+    n = 4096
+    rng = np.random.default_rng(5)
+    q = random_q(rng, 868)
+    a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
+    expect = oracle.rns_multiply(a, b, q)
+    with plan(n, q, 14) as p:
+        da = torch.from_numpy(a.view(np.int64)).cuda()
+        db = torch.from_numpy(b.view(np.int64)).cuda()
+        dc = torch.empty_like(da)
+        ws = torch.empty(p.workspace_bytes, dtype=torch.uint8, device="cuda")
+        s = torch.cuda.Stream()
+        p.multiply(da.data_ptr(), db.data_ptr(), dc.data_ptr(), ws.data_ptr(), s.cuda_stream)
+        s.synchronize()
+        assert (dc.cpu().numpy().view(np.uint64) == expect).all()
+        # plan-owned workspace on the default stream
+        dc.zero_()
+        p.multiply(da.data_ptr(), db.data_ptr(), dc.data_ptr())
+        torch.cuda.synchronize()
+        assert (dc.cpu().numpy().view(np.uint64) == expect).all()
+
+
+def test_full_size_linearity(cuda):
+    """Size-independent property at the benchmark size: (a1 + a2) b = a1 b + a2 b (mod q)."""
+    from tests.helpers import to_ints, from_ints
+    n = 32768
+    q = (1 << 868) - 11993087
+    rng = np.random.default_rng(21)
+    a1, a2, b = (uniform_below(rng, q, n, 14) for _ in range(3))
+    s = from_ints([(x + y) % q for x, y in zip(to_ints(a1), to_ints(a2))], 14)
+    with plan(n, q, 14) as p:
+        c1, c2, cs = p.multiply_host(a1, b), p.multiply_host(a2, b), p.multiply_host(s, b)
+    assert to_ints(cs) == [(x + y) % q for x, y in zip(to_ints(c1), to_ints(c2))]
