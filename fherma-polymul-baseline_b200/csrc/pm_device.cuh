@@ -1,13 +1,13 @@
-// Device arithmetic and the three fused passes of one negacyclic product.
+// The three fused passes of a negacyclic product, batched over products.
 //
 //   K1 convert_cols : wide coefficients -> residues mod every prime, then the
 //                     first log2(R) forward NTT stages ("column" stages, whose
 //                     butterflies span the R rows of an R x C view) done across
 //                     the lanes of a warp.
-//   K2 rows         : per (prime, row): the remaining forward stages of a and
-//                     b in registers + shared memory, the pointwise product,
-//                     and the first inverse stages -- one HBM read of a, b and
-//                     one write of the product per row.
+//   K2 rows         : per (product, prime, row): the remaining forward stages of
+//                     a and b in registers + shared memory, the pointwise
+//                     product, and the first inverse stages -- one read of a, b
+//                     and one write of the product per row.
 //   K3 cols_crt     : the last inverse stages across warp lanes, the CRT digit
 //                     t_i = r_i * N^-1 * (P/p_i)^-1, exact CRT accumulation,
 //                     fixed-point nearest quotient and the reduction mod q.
@@ -21,31 +21,44 @@
 //
 // Lazy ranges (Harvey): forward values stay in [0, 4p), inverse values in
 // [0, 2p); primes are below 2^30 so 4p fits a 32-bit word.
+//
+// Batch layout: product z reads a, b at io + z*io_bstride words, writes c
+// there too, and owns the residue planes at work + z*ws_bstride words
+// ([2][P][n] u32: plane 0 = a, then the product; plane 1 = b).
 #pragma once
 
 #include <cstdint>
 
+#include "crt_mac.cuh"
 #include "pm_common.cuh"
 
 namespace pm {
 
 // ---------------------------------------------------------------------------
 // K1: conversion + forward column stages (plain SIMT conversion).
-// grid (C/G, 2), block R*G threads; thread (g, r) owns coefficient r*C + col0 + g.
+// grid (C/G, 2*count, prime groups), block R*G threads; thread (g, r) owns
+// coefficient r*C + col0 + g.  Dynamic shared memory: ppc*W uint2 limb powers.
 // ---------------------------------------------------------------------------
 template <int W>
 __global__ void __launch_bounds__(256) k1_convert_cols(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
                                                        uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
                                                        const uint2* __restrict__ conv_pow,
                                                        const uint2* __restrict__ tw_fwd, int n, int logR, int logC,
-                                                       int P, int stride) {
+                                                       int P, int stride, int ppc, size_t io_bstride,
+                                                       size_t ws_bstride) {
+    extern __shared__ uint2 s_pow[];
     __shared__ uint32_t tile[256];
+    const int z = blockIdx.y >> 1, poly = blockIdx.y & 1;
+    const int i0 = blockIdx.z * ppc;
+    const int i1 = min(P, i0 + ppc);
+    for (int k = threadIdx.x; k < (i1 - i0) * W; k += blockDim.x)
+        s_pow[k] = __ldg(conv_pow + size_t(i0 + k / W) * kPowWords + k % W);
     const int R = 1 << logR;
     const int G = blockDim.x >> logR;
     const int r = threadIdx.x & (R - 1), g = threadIdx.x >> logR;
     const int col0 = blockIdx.x * G;
     const size_t J = (size_t(r) << logC) + col0 + g;
-    const uint32_t* src = (blockIdx.y ? b : a) + J * stride;
+    const uint32_t* src = (poly ? b : a) + z * io_bstride + J * stride;
     uint32_t x[W];
 #pragma unroll
     for (int k = 0; k < W; k += 2) {
@@ -55,14 +68,15 @@ __global__ void __launch_bounds__(256) k1_convert_cols(const uint32_t* __restric
         x[k + 1] = v.y;
     }
     const unsigned mask = blockDim.x >= 32 ? 0xffffffffu : ((1u << blockDim.x) - 1);
-    uint32_t* dst = res + size_t(blockIdx.y) * P * n;
+    uint32_t* dst = res + z * ws_bstride + size_t(poly) * P * n;
     const int t = threadIdx.x, tr = t / G, tg = t % G;
-    for (int i = 0; i < P; ++i) {
+    __syncthreads();
+    for (int i = i0; i < i1; ++i) {
         const PrimeConst pc = pcs[i];
-        const uint2* cp = conv_pow + i * kPowWords;
+        const uint2* cp = s_pow + (i - i0) * W;
         uint64_t acc = 0;
 #pragma unroll
-        for (int k = 0; k < W; ++k) acc += shoup_mul(x[k], __ldg(cp + k), pc.p);
+        for (int k = 0; k < W; ++k) acc += shoup_mul(x[k], cp[k], pc.p);
         uint32_t v = reduce60(acc, pc.p, pc.mu);
         const uint2* tw = tw_fwd + size_t(i) * kNMax;
         for (int s = 0; s < logR; ++s) {
@@ -85,7 +99,8 @@ __global__ void __launch_bounds__(256) k1_convert_cols(const uint32_t* __restric
 // of C = 2^LOGC values, 8 values per thread, T = C/8 threads per row:
 //   d = C >> (s0+K); for group m < 8>>K: gid = tid + T*m, blk = gid / d,
 //   o = gid % d; value l of the group sits at blk*(d<<K) + o + l*d.
-// Forward twiddle of stage s = s0+u for the value pair starting at l:
+// Twiddle of row stage s = s0+u for the value pair starting at l: the row-local
+// table entry 2^s + blk*2^u + (l >> (K-u)), which holds
 //   Psi_rev[(R + r) * 2^s + blk * 2^u + (l >> (K-u))].
 // ---------------------------------------------------------------------------
 template <int K>
@@ -114,18 +129,18 @@ __device__ __forceinline__ void pass_load(uint32_t (&v)[8], const uint32_t* s, i
 
 template <int K>
 __device__ __forceinline__ void pass_forward(uint32_t (&va)[8], uint32_t (&vb)[8], int tid, int T, int s0, int logd,
-                                             int rowbase, const uint2* __restrict__ tw, uint32_t p, uint32_t two_p) {
+                                             const uint2* tw, uint32_t p, uint32_t two_p) {
 #pragma unroll
     for (int m = 0; m < (8 >> K); ++m) {
         const int blk = (tid + T * m) >> logd;
 #pragma unroll
         for (int u = 0; u < K; ++u) {
             const int h = 1 << (K - 1 - u);
-            const uint2* tws = tw + ((rowbase << (s0 + u)) + (blk << u));
+            const uint2* tws = tw + ((1 << (s0 + u)) + (blk << u));
 #pragma unroll
             for (int l = 0; l < (1 << K); ++l) {
                 if (l & h) continue;
-                const uint2 w = __ldg(tws + (l >> (K - u)));
+                const uint2 w = tws[l >> (K - u)];
                 ct_bfly(va[(m << K) + l], va[(m << K) + l + h], w, p, two_p);
                 ct_bfly(vb[(m << K) + l], vb[(m << K) + l + h], w, p, two_p);
             }
@@ -134,50 +149,54 @@ __device__ __forceinline__ void pass_forward(uint32_t (&va)[8], uint32_t (&vb)[8
 }
 
 template <int K>
-__device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, int s0, int logd, int rowbase,
-                                             const uint2* __restrict__ tw, uint32_t p, uint32_t two_p) {
+__device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, int s0, int logd, const uint2* tw,
+                                             uint32_t p, uint32_t two_p) {
 #pragma unroll
     for (int m = 0; m < (8 >> K); ++m) {
         const int blk = (tid + T * m) >> logd;
 #pragma unroll
         for (int u = K - 1; u >= 0; --u) {
             const int h = 1 << (K - 1 - u);
-            const uint2* tws = tw + ((rowbase << (s0 + u)) + (blk << u));
+            const uint2* tws = tw + ((1 << (s0 + u)) + (blk << u));
 #pragma unroll
             for (int l = 0; l < (1 << K); ++l) {
                 if (l & h) continue;
-                const uint2 w = __ldg(tws + (l >> (K - u)));
+                const uint2 w = tws[l >> (K - u)];
                 gs_bfly(v[(m << K) + l], v[(m << K) + l + h], w, p, two_p);
             }
         }
     }
 }
 
-// Rows of C = 2^LOGC >= 8.  grid (R / rows_per_cta, P), block rows_per_cta * C/8.
-// Dynamic shared memory: rows_per_cta * 2 * C words.  The product overwrites
-// the a plane in place.
+constexpr int k2_threads(int logc) { return logc >= 12 ? 512 : (logc >= 11 ? 256 : 128); }
+constexpr int k2_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 3 : 7); }
+
+// Rows of C = 2^LOGC >= 8.  grid (R / rows_per_cta, P, count), block
+// rows_per_cta * C/8.  Dynamic shared memory per row: C uint2 forward and C
+// uint2 inverse twiddles, then 2C words of data.  The product overwrites the
+// a plane in place.
 template <int LOGC>
-__global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
-                                               const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv,
-                                               int n, int logR, int P) {
+__global__ void __launch_bounds__(k2_threads(LOGC), k2_min_blocks(LOGC))
+    k2_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
+            const uint2* __restrict__ tw_inv, int n, int logR, int P, size_t ws_bstride) {
     constexpr int C = 1 << LOGC;
     constexpr int T = C / 8;
     constexpr int NP3 = LOGC / 3;  // radix-8 passes
     constexpr int REM = LOGC % 3;  // stages of the closing pass
-    extern __shared__ uint32_t smem[];
+    extern __shared__ uint2 smem2[];
     const int sub = threadIdx.x / T, tid = threadIdx.x % T;
     const int rows_per_cta = blockDim.x / T;
     const int r = blockIdx.x * rows_per_cta + sub;
     const int i = blockIdx.y;
     const int R = 1 << logR;
-    uint32_t* sa = smem + sub * 2 * C;
+    uint2* stf = smem2 + sub * 2 * C;
+    uint2* sti = stf + C;
+    uint32_t* sa = reinterpret_cast<uint32_t*>(smem2 + rows_per_cta * 2 * C) + sub * 2 * C;
     uint32_t* sb = sa + C;
     const PrimeConst pc = pcs[i];
+    res += blockIdx.z * ws_bstride;
     uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
     const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
-    const uint2* twf = tw_fwd + size_t(i) * kNMax;
-    const uint2* twi = tw_inv + size_t(i) * kNMax;
-    const int rowbase = R + r;
 
     uint32_t va[8], vb[8];
 #pragma unroll
@@ -185,6 +204,19 @@ __global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const
         va[l] = ga[tid + l * T];
         vb[l] = gb[tid + l * T];
     }
+    // this row's twiddles: local entry j = 2^s + i' holds Psi_rev[(R + r) 2^s + i']
+    {
+        const uint2* gf = tw_fwd + size_t(i) * kNMax;
+        const uint2* gi = tw_inv + size_t(i) * kNMax;
+        for (int j = tid; j < C; j += T) {
+            if (j == 0) continue;
+            const int s = 31 - __clz(j);
+            const int gidx = ((R + r) << s) + (j - (1 << s));
+            stf[j] = __ldg(gf + gidx);
+            sti[j] = __ldg(gi + gidx);
+        }
+    }
+    __syncthreads();
     // forward radix-8 passes
 #pragma unroll
     for (int q3 = 0; q3 < NP3; ++q3) {
@@ -193,7 +225,7 @@ __global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const
             pass_load<3>(va, sa, tid, T, logd);
             pass_load<3>(vb, sb, tid, T, logd);
         }
-        pass_forward<3>(va, vb, tid, T, s0, logd, rowbase, twf, pc.p, pc.two_p);
+        pass_forward<3>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
         if (q3 + 1 < NP3 || REM) {
             __syncthreads();
             pass_store<3>(va, sa, tid, T, logd);
@@ -205,7 +237,7 @@ __global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const
         const int s0 = 3 * NP3, logd = 0;
         pass_load<REM>(va, sa, tid, T, logd);
         pass_load<REM>(vb, sb, tid, T, logd);
-        pass_forward<REM>(va, vb, tid, T, s0, logd, rowbase, twf, pc.p, pc.two_p);
+        pass_forward<REM>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
     }
     // pointwise product, operands reduced to [0, p)
 #pragma unroll
@@ -216,7 +248,7 @@ __global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const
     }
     if constexpr (REM > 0) {
         const int s0 = 3 * NP3, logd = 0;
-        pass_inverse<REM>(va, tid, T, s0, logd, rowbase, twi, pc.p, pc.two_p);
+        pass_inverse<REM>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
         __syncthreads();
         pass_store<REM>(va, sa, tid, T, logd);
         __syncthreads();
@@ -225,7 +257,7 @@ __global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const
     for (int q3 = NP3 - 1; q3 >= 0; --q3) {
         const int s0 = 3 * q3, logd = LOGC - s0 - 3;
         if (q3 + 1 < NP3 || REM) pass_load<3>(va, sa, tid, T, logd);
-        pass_inverse<3>(va, tid, T, s0, logd, rowbase, twi, pc.p, pc.two_p);
+        pass_inverse<3>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
         if (q3 > 0) {
             __syncthreads();
             pass_store<3>(va, sa, tid, T, logd);
@@ -237,14 +269,16 @@ __global__ void __launch_bounds__(256) k2_rows(uint32_t* __restrict__ res, const
 }
 
 // Rows of C <= 4 (N <= 128): one thread per row, everything in registers.
-__global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
+// grid ((R+31)/32, P, count).
+static __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs,
                               const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv, int n, int logR,
-                              int logC, int P) {
+                              int logC, int P, size_t ws_bstride) {
     const int R = 1 << logR, C = 1 << logC;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (r >= R) return;
     const PrimeConst pc = pcs[i];
+    res += blockIdx.z * ws_bstride;
     uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
     const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
     const uint2* twf = tw_fwd + size_t(i) * kNMax;
@@ -261,7 +295,7 @@ __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeConst* __re
         for (int j = 0; j < 4; ++j)
             if (j < C && !(j & t)) {
                 const uint2 w = twf[((R + r) << s) + (j >> (logC - s))];
-                // indices are compile-time after unrolling; t is runtime, select explicitly
+                // register indices must be compile-time; select the partner explicitly
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
                     if (k == j + t) {
@@ -294,21 +328,9 @@ __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeConst* __re
 
 // ---------------------------------------------------------------------------
 // Multiprecision tail of the CRT, per coefficient, all in registers.
-// acc: W+2 columns of 64-bit deferred-carry sums.
-// ---------------------------------------------------------------------------
-template <int W>
-__device__ __forceinline__ void normalize(uint64_t (&acc)[W + 2]) {
-    uint64_t carry = 0;
-#pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
-        const uint64_t v = acc[k] + carry;
-        acc[k] = v & 0xffffffffull;
-        carry = v >> 32;
-    }
-}
-
 // v (W+2 words) mod q, v < 2^(sbits+37); q has sbits bits and W words;
-// mu_q = floor(2^(sbits+62) / q).  Writes W words of the canonical residue.
+// mu_q = floor(2^(sbits+62) / q).  Leaves the canonical residue in v[0..W).
+// ---------------------------------------------------------------------------
 template <int W>
 __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q, uint64_t mu_q,
                                              int sbits) {
@@ -357,9 +379,30 @@ __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_
     }
 }
 
+// Final CRT step shared by the SIMT and tensor paths: v = acc + nearest *
+// (-P mod q), reduce mod q, store one coefficient (stride words).
+template <int W>
+__device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t nearest, const uint32_t* s_q,
+                                           uint64_t mu_q, int sbits, uint32_t* dst, int stride) {
+    uint32_t carry = 0;
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        const uint64_t x = uint64_t(v[k]) + (k < W ? uint64_t(s_q[W + k]) * nearest : 0) + carry;
+        v[k] = uint32_t(x);
+        carry = uint32_t(x >> 32);
+    }
+    reduce_mod_q<W>(v, s_q, mu_q, sbits);
+#pragma unroll
+    for (int k = 0; k < W; k += 2)
+        if (k < stride) *reinterpret_cast<uint2*>(dst + k) = make_uint2(v[k], v[k + 1]);
+    for (int k = W; k < stride; ++k) dst[k] = 0;
+}
+
 // ---------------------------------------------------------------------------
 // K3: inverse column stages + CRT (plain SIMT accumulation).
-// grid (C/G), block R*G; dynamic shared memory P*W words ((P/p_i) mod q rows).
+// grid (C/G, count), block R*G.  Dynamic shared memory: P*W words of
+// (P/p_i) mod q rows, then P*R*G words holding every prime's residue tile,
+// loaded up front so all loads are in flight at once.
 // consts = q[W] followed by (-P mod q)[W].
 // ---------------------------------------------------------------------------
 template <int W>
@@ -368,27 +411,31 @@ __global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ 
                                                    const uint2* __restrict__ tw_inv, const uint2* __restrict__ scale,
                                                    const uint32_t* __restrict__ mq,
                                                    const uint32_t* __restrict__ consts, uint64_t mu_q, int sbits,
-                                                   int n, int logR, int logC, int P, int stride) {
-    extern __shared__ uint32_t s_mq[];
-    __shared__ uint32_t tile[256];
+                                                   int n, int logR, int logC, int P, int stride, size_t io_bstride,
+                                                   size_t ws_bstride) {
+    extern __shared__ uint32_t sm3[];
     __shared__ uint32_t s_q[2 * W];
-    for (int k = threadIdx.x; k < P * W; k += blockDim.x) s_mq[k] = mq[k];
-    for (int k = threadIdx.x; k < 2 * W; k += blockDim.x) s_q[k] = consts[k];
+    const int RG = blockDim.x;
+    uint32_t* s_mq = sm3;
+    uint32_t* tiles = sm3 + P * W;
     const int R = 1 << logR;
     const int G = blockDim.x >> logR;
     const int r = threadIdx.x & (R - 1), g = threadIdx.x >> logR;
     const int col0 = blockIdx.x * G;
     const int t = threadIdx.x, tr = t / G, tg = t % G;
+    res += blockIdx.y * ws_bstride;
+    out += blockIdx.y * io_bstride;
+    for (int k = threadIdx.x; k < P * W; k += blockDim.x) s_mq[k] = mq[k];
+    for (int k = threadIdx.x; k < 2 * W; k += blockDim.x) s_q[k] = consts[k];
+    for (int i = 0; i < P; ++i) tiles[i * RG + t] = res[size_t(i) * n + (size_t(tr) << logC) + col0 + tg];
+    __syncthreads();
     const unsigned mask = blockDim.x >= 32 ? 0xffffffffu : ((1u << blockDim.x) - 1);
-    uint64_t acc[W + 2];
+    uint32_t acc[W + 2];
 #pragma unroll
     for (int k = 0; k < W + 2; ++k) acc[k] = 0;
     uint64_t f0 = 0, f1 = 0;
     for (int i = 0; i < P; ++i) {
-        __syncthreads();
-        tile[t] = res[size_t(i) * n + (size_t(tr) << logC) + col0 + tg];
-        __syncthreads();
-        uint32_t v = tile[r * G + g];
+        uint32_t v = tiles[i * RG + r * G + g];
         const PrimeConst pc = pcs[i];
         const uint2* tw = tw_inv + size_t(i) * kNMax;
         for (int s = logR - 1; s >= 0; --s) {
@@ -403,36 +450,22 @@ __global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ 
             }
         }
         const uint32_t ti = csub(shoup_mul(v, __ldg(scale + i), pc.p), pc.p);
-        const uint32_t* m = s_mq + i * W;
+        uint32_t m[W];
 #pragma unroll
-        for (int k = 0; k < W; ++k) acc[k] += uint64_t(ti) * m[k];
+        for (int k = 0; k < W; ++k) m[k] = s_mq[i * W + k];
+        crt_mac<W>(acc, ti, m);
         f0 += uint64_t(ti) * uint32_t(pc.recip);
         f1 += uint64_t(ti) * uint32_t(pc.recip >> 32);
         if ((i & 3) == 3) {
-            normalize<W>(acc);
             f1 += f0 >> 32;
             f0 &= 0xffffffffull;
         }
     }
-    normalize<W>(acc);
     f1 += f0 >> 32;
-    // nearest integer of sum t_i / p_i  (fraction carried in f1:f0 / 2^64)
+    // nearest integer of sum t_i / p_i (the fraction is f1:f0 / 2^64)
     const uint32_t nearest = uint32_t((f1 + (1ull << 31)) >> 32);
-    uint32_t v[W + 2];
-    uint64_t carry = 0;
-#pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
-        const uint64_t x = acc[k] + (k < W ? uint64_t(s_q[W + k]) * nearest : 0) + carry;
-        v[k] = uint32_t(x);
-        carry = x >> 32;
-    }
-    reduce_mod_q<W>(v, s_q, mu_q, sbits);
     const size_t J = (size_t(r) << logC) + col0 + g;
-    uint32_t* dst = out + J * stride;
-#pragma unroll
-    for (int k = 0; k < W; k += 2)
-        if (k < stride) *reinterpret_cast<uint2*>(dst + k) = make_uint2(v[k], v[k + 1]);
-    for (int k = W; k < stride; ++k) dst[k] = 0;
+    crt_finish<W>(acc, nearest, s_q, mu_q, sbits, out + J * stride, stride);
 }
 
 }  // namespace pm

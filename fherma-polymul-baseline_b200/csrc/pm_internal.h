@@ -66,6 +66,8 @@ struct PlanCore {
     uint32_t* d_consts = nullptr;  // q[W], (-P_total mod q)[W]
     uint2* d_scale = nullptr;      // [P] n^-1 (P_total/p_i)^-1 mod p_i
     uint32_t* d_work = nullptr;    // [2][P][n] residue planes (plan-owned workspace)
+    void* d_batch_work = nullptr;  // residue planes for a group of products (pm_multiply_batch)
+    uint32_t batch_work_group = 0;
     size_t workspace_bytes = 0;
     size_t io_bytes = 0;           // bytes of one polynomial
     void* d_io = nullptr;          // a, b, c device copies for the host-buffer call
@@ -73,14 +75,21 @@ struct PlanCore {
     cudaStream_t stream = nullptr;
     // tensor path constants
     uint8_t* d_crt_weights = nullptr;
+    uint32_t* d_err = nullptr;     // set by a kernel whose bounded wait ran out
     uint32_t tensor_k_crt = 0;
 
     void init(uint32_t n, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs, uint32_t flags);
+    void ensure_batch_workspace(uint32_t group);
     ~PlanCore();
 };
 
 void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
-                 cudaStream_t st);
+                 uint32_t count, cudaStream_t st);
+uint32_t group_size(const PlanCore& s);
+void launch_rows(const PlanCore& s, uint32_t* work, uint32_t count, cudaStream_t st);
+void check_device_errors(const PlanCore& s);
+void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
+                  uint32_t group, void* workspace, cudaStream_t st);
 void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                     cudaStream_t st);
 void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c);
@@ -89,6 +98,6 @@ void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* 
 void tensor_init(PlanCore& s);
 void tensor_release(PlanCore& s);
 void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
-                   cudaStream_t st);
+                   uint32_t count, cudaStream_t st);
 
 }  // namespace pm

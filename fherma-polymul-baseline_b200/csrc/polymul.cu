@@ -255,7 +255,9 @@ PlanCore::~PlanCore() {
     cudaFree(d_mq);
     cudaFree(d_consts);
     cudaFree(d_scale);
+    tensor_release(*this);
     cudaFree(d_work);
+    cudaFree(d_batch_work);
     cudaFree(d_io);
     cudaFreeHost(h_stage);
     if (stream) cudaStreamDestroy(stream);
@@ -282,7 +284,10 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     n = n_;
     logn = 0;
     while ((1u << logn) < n) ++logn;
-    logR = logn < 5 ? logn : 5;
+    // rows of the R x C view: 32 for the SIMT path (column stages across warp
+    // lanes), 16 for the tensor path (column stages in registers)
+    const uint32_t maxlogR = (flags_ & PM_CONVERT_TENSOR) ? 4 : 5;
+    logR = logn < maxlogR ? logn : maxlogR;
     logC = logn - logR;
     coef_limbs = coef_limbs_;
     stride = 2 * coef_limbs;
@@ -336,59 +341,85 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     if (flags & PM_CONVERT_TENSOR) tensor_init(*this);
 }
 
+void PlanCore::ensure_batch_workspace(uint32_t group) {
+    if (batch_work_group >= group) return;
+    cuda_check(cudaStreamSynchronize(stream), "drain plan stream");
+    cudaFree(d_batch_work);
+    d_batch_work = nullptr;
+    batch_work_group = 0;
+    cuda_check(cudaMalloc(&d_batch_work, workspace_bytes * group), "allocate batch workspace");
+    batch_work_group = group;
+}
+
 // ---------------------------------------------------------------------------
 // launch sequence of one product: K1 -> K2 -> K3 on one stream
 // ---------------------------------------------------------------------------
 namespace {
+struct Batch {
+    uint32_t count;     // products in this launch
+    size_t io_bstride;  // words between consecutive products' a (b, c)
+    size_t ws_bstride;  // words between consecutive products' residue planes
+};
+
 template <int W>
-void launch_k1(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, cudaStream_t st) {
+void launch_k1(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, const Batch& bt,
+               cudaStream_t st) {
     const int G = s.logC >= 3 ? 8 : (1 << s.logC);
-    dim3 grid((1u << s.logC) / G, 2), block((1u << s.logR) * G);
-    k1_convert_cols<W><<<grid, block, 0, st>>>(a, b, work, s.basis->d_pc, s.basis->d_conv_pow, s.basis->d_tw_fwd,
-                                                int(s.n), int(s.logR), int(s.logC), int(s.P), int(s.stride));
+    const int groups = s.P >= 32 ? 4 : (s.P >= 16 ? 2 : 1);
+    const int ppc = int((s.P + groups - 1) / groups);
+    dim3 grid((1u << s.logC) / G, 2 * bt.count, (s.P + ppc - 1) / ppc), block((1u << s.logR) * G);
+    const size_t smem = size_t(ppc) * W * sizeof(uint2);
+    k1_convert_cols<W><<<grid, block, smem, st>>>(a, b, work, s.basis->d_pc, s.basis->d_conv_pow, s.basis->d_tw_fwd,
+                                                  int(s.n), int(s.logR), int(s.logC), int(s.P), int(s.stride), ppc,
+                                                  bt.io_bstride, bt.ws_bstride);
 }
 
 template <int W>
-void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, cudaStream_t st) {
+void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, const Batch& bt, cudaStream_t st) {
     const int G = s.logC >= 3 ? 8 : (1 << s.logC);
-    dim3 grid((1u << s.logC) / G), block((1u << s.logR) * G);
-    const size_t smem = size_t(s.P) * W * 4;
+    const int RG = (1 << s.logR) * G;
+    dim3 grid((1u << s.logC) / G, bt.count), block(RG);
+    const size_t smem = (size_t(s.P) * W + size_t(s.P) * RG) * 4;
+    if (smem > 48 * 1024)
+        cuda_check(cudaFuncSetAttribute(k3_cols_crt<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                   "raise K3 shared memory");
     k3_cols_crt<W><<<grid, block, smem, st>>>(work, c, s.basis->d_pc, s.basis->d_tw_inv, s.d_scale, s.d_mq,
-                                              s.d_consts, s.mu_q, int(s.qbits), int(s.n), int(s.logR),
-                                              int(s.logC), int(s.P), int(s.stride));
+                                              s.d_consts, s.mu_q, int(s.qbits), int(s.n), int(s.logR), int(s.logC),
+                                              int(s.P), int(s.stride), bt.io_bstride, bt.ws_bstride);
 }
 
 template <int LOGC>
-void launch_k2_fixed(const PlanCore& s, uint32_t* work, cudaStream_t st) {
+void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
     constexpr int C = 1 << LOGC, T = C / 8;
     int rows = T >= 128 ? 1 : 128 / T;
     const int R = 1 << s.logR;
     if (rows > R) rows = R;
-    const size_t smem = size_t(rows) * 2 * C * 4;
+    const size_t smem = size_t(rows) * 24 * C;  // 2C uint2 twiddles + 2C words of data per row
     if (smem > 48 * 1024)
         cuda_check(cudaFuncSetAttribute(k2_rows<LOGC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "raise K2 shared memory");
-    dim3 grid(R / rows, s.P), block(rows * T);
+    dim3 grid(R / rows, s.P, bt.count), block(rows * T);
     k2_rows<LOGC><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.n),
-                                             int(s.logR), int(s.P));
+                                             int(s.logR), int(s.P), bt.ws_bstride);
 }
 
-void launch_k2(const PlanCore& s, uint32_t* work, cudaStream_t st) {
+void launch_k2(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
     switch (s.logC) {
-        case 3: return launch_k2_fixed<3>(s, work, st);
-        case 4: return launch_k2_fixed<4>(s, work, st);
-        case 5: return launch_k2_fixed<5>(s, work, st);
-        case 6: return launch_k2_fixed<6>(s, work, st);
-        case 7: return launch_k2_fixed<7>(s, work, st);
-        case 8: return launch_k2_fixed<8>(s, work, st);
-        case 9: return launch_k2_fixed<9>(s, work, st);
-        case 10: return launch_k2_fixed<10>(s, work, st);
-        case 11: return launch_k2_fixed<11>(s, work, st);
+        case 12: return launch_k2_fixed<12>(s, work, bt, st);
+        case 3: return launch_k2_fixed<3>(s, work, bt, st);
+        case 4: return launch_k2_fixed<4>(s, work, bt, st);
+        case 5: return launch_k2_fixed<5>(s, work, bt, st);
+        case 6: return launch_k2_fixed<6>(s, work, bt, st);
+        case 7: return launch_k2_fixed<7>(s, work, bt, st);
+        case 8: return launch_k2_fixed<8>(s, work, bt, st);
+        case 9: return launch_k2_fixed<9>(s, work, bt, st);
+        case 10: return launch_k2_fixed<10>(s, work, bt, st);
+        case 11: return launch_k2_fixed<11>(s, work, bt, st);
         default: {
             const int R = 1 << s.logR;
-            dim3 grid((R + 31) / 32, s.P), block(R < 32 ? R : 32);
+            dim3 grid((R + 31) / 32, s.P, bt.count), block(R < 32 ? R : 32);
             k2_rows_small<<<grid, block, 0, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
-                                                 int(s.n), int(s.logR), int(s.logC), int(s.P));
+                                                 int(s.n), int(s.logR), int(s.logC), int(s.P), bt.ws_bstride);
         }
     }
 }
@@ -406,21 +437,26 @@ void launch_k2(const PlanCore& s, uint32_t* work, cudaStream_t st) {
     }
 }  // namespace
 
+void launch_rows(const PlanCore& s, uint32_t* work, uint32_t count, cudaStream_t st) {
+    launch_k2(s, work, Batch{count, size_t(s.n) * s.stride, s.workspace_bytes / 4}, st);
+}
+
 void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
-                 cudaStream_t st) {
+                 uint32_t count, cudaStream_t st) {
+    const Batch bt{count, size_t(s.n) * s.stride, s.workspace_bytes / 4};
     {
         ProfileScope prof("k1_convert_cols", st);
-#define PM_K1(W) launch_k1<W>(s, a, b, work, st)
+#define PM_K1(W) launch_k1<W>(s, a, b, work, bt, st)
         PM_DISPATCH_W(s.W, PM_K1)
 #undef PM_K1
     }
     {
         ProfileScope prof("k2_rows", st);
-        launch_k2(s, work, st);
+        launch_k2(s, work, bt, st);
     }
     {
         ProfileScope prof("k3_cols_crt", st);
-#define PM_K3(W) launch_k3<W>(s, work, c, st)
+#define PM_K3(W) launch_k3<W>(s, work, c, bt, st)
         PM_DISPATCH_W(s.W, PM_K3)
 #undef PM_K3
     }
@@ -428,16 +464,46 @@ void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32
     count_launches(3);
 }
 
+// A kernel that gave up a bounded wait records it in the plan's error word.
+void check_device_errors(const PlanCore& s) {
+    if (!s.d_err) return;
+    uint32_t err = 0;
+    cuda_check(cudaMemcpy(&err, s.d_err, sizeof err, cudaMemcpyDeviceToHost), "read error word");
+    if (err) {
+        cudaMemset(s.d_err, 0, sizeof err);
+        throw Failure(PM_ERR_TIMEOUT, "a tensor-core wait timed out; results of that call are invalid");
+    }
+}
+
+// Products whose residue planes fit in about 64 MB run together, so the
+// planes K1 writes are still in L2 when K2 and K3 read them.
+uint32_t group_size(const PlanCore& s) {
+    const size_t budget = size_t(64) << 20;
+    size_t g = budget / s.workspace_bytes;
+    if (g < 1) g = 1;
+    if (g > 64) g = 64;
+    return uint32_t(g);
+}
+
+void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
+                  uint32_t group, void* workspace, cudaStream_t st) {
+    uint32_t* work = static_cast<uint32_t*>(workspace);
+    const size_t io_words = size_t(s.n) * s.stride;
+    for (uint32_t z = 0; z < count; z += group) {
+        const uint32_t g = count - z < group ? count - z : group;
+        const uint32_t* a32 = reinterpret_cast<const uint32_t*>(a) + z * io_words;
+        const uint32_t* b32 = reinterpret_cast<const uint32_t*>(b) + z * io_words;
+        uint32_t* c32 = reinterpret_cast<uint32_t*>(c) + z * io_words;
+        if (s.flags & PM_CONVERT_TENSOR)
+            launch_tensor(s, a32, b32, c32, work, g, st);
+        else
+            launch_simt(s, a32, b32, c32, work, g, st);
+    }
+}
+
 void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                     cudaStream_t st) {
-    uint32_t* work = workspace ? static_cast<uint32_t*>(workspace) : s.d_work;
-    const uint32_t* a32 = reinterpret_cast<const uint32_t*>(a);
-    const uint32_t* b32 = reinterpret_cast<const uint32_t*>(b);
-    uint32_t* c32 = reinterpret_cast<uint32_t*>(c);
-    if (s.flags & PM_CONVERT_TENSOR)
-        launch_tensor(s, a32, b32, c32, work, st);
-    else
-        launch_simt(s, a32, b32, c32, work, st);
+    launch_batch(s, a, b, c, 1, 1, workspace ? workspace : s.d_work, st);
 }
 
 // Host buffers: pinned memory is copied directly; pageable memory is staged
@@ -477,6 +543,7 @@ void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* 
     cuda_check(cudaMemcpyAsync(dst, dev + 2 * s.io_bytes, s.io_bytes, cudaMemcpyDeviceToHost, s.stream),
                "copy c to host");
     cuda_check(cudaStreamSynchronize(s.stream), "product");
+    check_device_errors(s);
     if (!pc) std::memcpy(c, stage + 2 * s.io_bytes, s.io_bytes);
 }
 
@@ -540,6 +607,33 @@ extern "C" int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, 
                            pm_stream stream) {
     if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
     PM_GUARD(pm::launch_product(plan->core, a, b, c, workspace, reinterpret_cast<cudaStream_t>(stream)))
+}
+
+extern "C" int pm_batch_workspace_size(const pm_plan* plan, uint32_t count, size_t* bytes) {
+    if (!plan || !bytes) return fail(PM_ERR_INVALID, "NULL argument");
+    const uint32_t g = pm::group_size(plan->core);
+    *bytes = plan->core.workspace_bytes * (count < g ? (count ? count : 1) : g);
+    return PM_OK;
+}
+
+extern "C" int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
+                                 void* workspace, size_t workspace_bytes, pm_stream stream) {
+    if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
+    if (count == 0) return PM_OK;
+    PM_GUARD({
+        auto& s = plan->core;
+        uint32_t g = pm::group_size(s);
+        if (g > count) g = count;
+        if (workspace) {
+            const size_t fit = workspace_bytes / s.workspace_bytes;
+            if (fit == 0) throw Failure(PM_ERR_INVALID, "workspace smaller than one product needs");
+            if (fit < g) g = uint32_t(fit);
+        } else {
+            s.ensure_batch_workspace(g);
+            workspace = s.d_batch_work;
+        }
+        pm::launch_batch(s, a, b, c, count, g, workspace, reinterpret_cast<cudaStream_t>(stream));
+    })
 }
 
 extern "C" int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c) {

@@ -56,6 +56,8 @@ def lib():
         L.pm_plan_destroy.argtypes = [vp]
         L.pm_multiply.argtypes = [vp, vp, vp, vp, vp, vp]
         L.pm_multiply_host.argtypes = [vp, vp, vp, vp]
+        L.pm_multiply_batch.argtypes = [vp, vp, vp, vp, u32, vp, ctypes.c_size_t, vp]
+        L.pm_batch_workspace_size.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_size_t)]
         L.pm_basis_query.argtypes = [u32, u32, ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
         L.pm_status_string.restype = ctypes.c_char_p
         L.pm_status_string.argtypes = [ctypes.c_int]
@@ -158,6 +160,16 @@ class Plan:
         c = np.empty_like(a) if out is None else out
         check(lib().pm_multiply_host(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
         return c
+
+    def multiply_batch(self, a_ptr, b_ptr, c_ptr, count, workspace=0, workspace_bytes=0, stream=0):
+        """count products stored back to back on the device (asynchronous)."""
+        check(lib().pm_multiply_batch(self._h, a_ptr, b_ptr, c_ptr, count, workspace or None, workspace_bytes,
+                                      stream or None))
+
+    def batch_workspace_size(self, count):
+        out = ctypes.c_size_t(0)
+        check(lib().pm_batch_workspace_size(self._h, count, ctypes.byref(out)))
+        return out.value
 
     def multiply(self, a_ptr, b_ptr, c_ptr, workspace=0, stream=0):
         """Asynchronous product on device pointers (ints) on a CUDA stream handle."""

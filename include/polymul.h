@@ -81,6 +81,20 @@ int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c
                 pm_stream stream);
 
 /*
+ * A batch of `count` products of one plan, stored back to back: a, b, c are
+ * device arrays [count][n][coef_limbs].  The library runs them in groups whose
+ * residue planes fit in L2, so the three passes of a group hand their planes
+ * to each other on-chip.  workspace: a device buffer of workspace_bytes (at
+ * least one product's worth; more allows larger groups, see
+ * pm_batch_workspace_size), or NULL to use a plan-owned buffer that the first
+ * call allocates.  Asynchronous on `stream`.
+ */
+int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
+                      void* workspace, size_t workspace_bytes, pm_stream stream);
+/* Workspace bytes pm_multiply_batch uses for `count` products at its preferred group size. */
+int pm_batch_workspace_size(const pm_plan* plan, uint32_t count, size_t* bytes);
+
+/*
  * One product on host memory, synchronous: copy in, multiply, copy out.
  * Pinned (page-locked) buffers are copied directly; pageable ones are staged
  * through the plan's pinned buffers.  Replaces fherma_run (fherma.h:45;

@@ -1,4 +1,5 @@
-"""GPU parity of the plain (SIMT conversion/CRT) path through the C ABI.
+"""GPU parity through the C ABI, for both conversion/CRT paths: the plain
+SIMT one and the tcgen05 INT8 tensor-core one (the NTT kernels are shared).
 
 Bit-exact: every product must equal the oracle's canonical residue in [0, q).
 The reference's golden points (tests/golden/golden.json, produced by its own
@@ -15,53 +16,56 @@ from tests.helpers import random_q, uniform_below
 
 pytestmark = pytest.mark.gpu
 
-TENSOR = False
+
+@pytest.fixture(params=["simt", "tensor"])
+def path(request):
+    return request.param
 
 
-def plan(n, q, limbs=None):
-    return polymul.Plan(n, q, coef_limbs=limbs, tensor=TENSOR)
+def make_plan(path, n, q, limbs=None):
+    return polymul.Plan(n, q, coef_limbs=limbs, tensor=(path == "tensor"))
 
 
-def test_golden_points(cuda, golden):
+def test_golden_points(cuda, golden, path):
     for point in golden["points"]:
         q = int(point["q"], 16)
-        with plan(point["N"], q, 14) as p:
+        with make_plan(path, point["N"], q, 14) as p:
             for label, a, b, rec in point_cases(point):  # same plan reused across cases
                 c = p.multiply_host(a, b)
                 assert sha(c.tobytes()) == rec["c_sha256"], (point["N"], point["delta"], label)
 
 
 @pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 64, 128, 256, 512, 2048, 8192, 16384, 65536])
-def test_ring_sizes_868(cuda, n):
+def test_ring_sizes_868(cuda, path, n):
     rng = np.random.default_rng(n)
     q = random_q(rng, 868)
     a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
-    with plan(n, q, 14) as p:
+    with make_plan(path, n, q, 14) as p:
         assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
 
 
 @pytest.mark.parametrize("bits", [3, 31, 64, 65, 129, 200, 257, 384, 517, 640, 700, 800, 867, 896])
-def test_widths(cuda, bits):
+def test_widths(cuda, path, bits):
     n = 1024
     rng = np.random.default_rng(bits)
     q = random_q(rng, bits)
     a, b = uniform_below(rng, q, n), uniform_below(rng, q, n)
-    with plan(n, q) as p:
+    with make_plan(path, n, q) as p:
         assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
 
 
-def test_padded_limbs(cuda):
+def test_padded_limbs(cuda, path):
     """Coefficients stored wider than q needs (the fherma layout keeps 28 words for any q)."""
     rng = np.random.default_rng(3)
     q = random_q(rng, 200)
     a, b = uniform_below(rng, q, 256, 14), uniform_below(rng, q, 256, 14)
-    with plan(256, q, 14) as p:
+    with make_plan(path, 256, q, 14) as p:
         c = p.multiply_host(a, b)
     assert (c == oracle.rns_multiply(a, b, q)).all()
     assert not c[:, 4:].any()
 
 
-def test_edge_values_full_size(cuda):
+def test_edge_values_full_size(cuda, path):
     n = 32768
     q = (1 << 868) - 1  # not prime: any odd q is accepted
     vals = [0, 1, q - 1, q - 2, 1 << 864, (1 << 864) - 1, 1 << 32, (1 << 32) - 1, (1 << 867), 2]
@@ -70,18 +74,18 @@ def test_edge_values_full_size(cuda):
     from tests.helpers import from_ints
     a = from_ints([vals[i] for i in idx], 14)
     b = from_ints([vals[i] for i in rng.permutation(idx)], 14)
-    with plan(n, q, 14) as p:
+    with make_plan(path, n, q, 14) as p:
         assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
 
 
-def test_device_pointers_and_external_workspace(cuda):
+def test_device_pointers_and_external_workspace(cuda, path):
     torch = cuda
     n = 4096
     rng = np.random.default_rng(5)
     q = random_q(rng, 868)
     a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
     expect = oracle.rns_multiply(a, b, q)
-    with plan(n, q, 14) as p:
+    with make_plan(path, n, q, 14) as p:
         da = torch.from_numpy(a.view(np.int64)).cuda()
         db = torch.from_numpy(b.view(np.int64)).cuda()
         dc = torch.empty_like(da)
@@ -97,7 +101,7 @@ def test_device_pointers_and_external_workspace(cuda):
         assert (dc.cpu().numpy().view(np.uint64) == expect).all()
 
 
-def test_full_size_linearity(cuda):
+def test_full_size_linearity(cuda, path):
     """Size-independent property at the benchmark size: (a1 + a2) b = a1 b + a2 b (mod q)."""
     from tests.helpers import to_ints, from_ints
     n = 32768
@@ -105,6 +109,58 @@ def test_full_size_linearity(cuda):
     rng = np.random.default_rng(21)
     a1, a2, b = (uniform_below(rng, q, n, 14) for _ in range(3))
     s = from_ints([(x + y) % q for x, y in zip(to_ints(a1), to_ints(a2))], 14)
-    with plan(n, q, 14) as p:
+    with make_plan(path, n, q, 14) as p:
         c1, c2, cs = p.multiply_host(a1, b), p.multiply_host(a2, b), p.multiply_host(s, b)
     assert to_ints(cs) == [(x + y) % q for x, y in zip(to_ints(c1), to_ints(c2))]
+
+
+@pytest.mark.parametrize("n,bits,count", [(32768, 868, 7), (1024, 300, 33), (64, 868, 5), (65536, 868, 3)])
+def test_batch_api(cuda, path, n, bits, count):
+    """pm_multiply_batch: products back to back, a count that is not a multiple of the group size."""
+    torch = cuda
+    rng = np.random.default_rng(n + count)
+    q = random_q(rng, bits)
+    limbs = (bits + 63) // 64
+    a = np.stack([uniform_below(rng, q, n, limbs) for _ in range(count)])
+    b = np.stack([uniform_below(rng, q, n, limbs) for _ in range(count)])
+    with make_plan(path, n, q, limbs) as p:
+        da = torch.from_numpy(a.view(np.int64)).cuda()
+        db = torch.from_numpy(b.view(np.int64)).cuda()
+        dc = torch.zeros_like(da)
+        p.multiply_batch(da.data_ptr(), db.data_ptr(), dc.data_ptr(), count)
+        torch.cuda.synchronize()
+        got = dc.cpu().numpy().view(np.uint64)
+        # caller workspace of exactly one product forces groups of one
+        dc2 = torch.zeros_like(da)
+        ws = torch.empty(p.workspace_bytes, dtype=torch.uint8, device="cuda")
+        p.multiply_batch(da.data_ptr(), db.data_ptr(), dc2.data_ptr(), count, ws.data_ptr(), p.workspace_bytes)
+        torch.cuda.synchronize()
+        assert (dc2.cpu().numpy().view(np.uint64) == got).all()
+    for k in sorted({0, count // 2, count - 1}):
+        assert (got[k] == oracle.rns_multiply(a[k], b[k], q)).all(), k
+
+
+def test_conversion_byte_edges(cuda, path):
+    """Coefficients made of 0x00 / 0xFF / 0x80 / 0x7F bytes, the extremes of the
+    INT8 digit contraction (the reference checks the same bytes in
+    tests/tensor_conversion.cpp:12)."""
+    n = 4096
+    q = (1 << 868) - 1
+    from tests.helpers import from_ints
+    patterns = [0, q - 1, int.from_bytes(b"\x80" * 108, "little"), int.from_bytes(b"\x7f" * 108, "little"),
+                int.from_bytes(b"\xff" * 108, "little"), (1 << 864) - 1]
+    rng = np.random.default_rng(99)
+    a = from_ints([patterns[i] for i in rng.integers(0, len(patterns), size=n)], 14)
+    b = from_ints([patterns[i] for i in rng.integers(0, len(patterns), size=n)], 14)
+    with make_plan(path, n, q, 14) as p:
+        assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
+
+
+def test_paths_agree_bitwise(cuda):
+    """The tensor path is bit-exact against the plain path on the same inputs."""
+    n = 32768
+    rng = np.random.default_rng(4242)
+    q = random_q(rng, 868)
+    a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
+    with make_plan("simt", n, q, 14) as p1, make_plan("tensor", n, q, 14) as p2:
+        assert (p1.multiply_host(a, b) == p2.multiply_host(a, b)).all()
