@@ -19,10 +19,13 @@
 // after a shared-memory transpose.  Operands are staged by the threads into
 // the canonical K-major 128-byte-swizzled layout; one thread issues the MMAs;
 // completion is signalled through an mbarrier with a bounded wait.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/polymul.h"
@@ -129,6 +132,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// 4-D tiled TMA load into shared memory, completion counted on `bar` (no multicast)
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // byte offset of (row m, byte k < 128) inside one 128-byte-swizzled atom column
 __host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t m, uint32_t k) {
     return (m >> 3) * 1024 + (m & 7) * 128 + ((((k >> 4) ^ (m & 7)) & 7) << 4) + (k & 15);
@@ -138,27 +156,29 @@ __host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t m, uint32_t k
 
 // ---------------------------------------------------------------------------
 // K1T: tensor-core conversion + forward column stages.
-// grid (ctas, prime groups); block 128.  CTA (x, pg) converts the coefficients
-// of tiles x, x + ctas, ... for the 16 primes of group pg.  Tile index ->
-// (product z, polynomial, column group cg); the tile holds coefficient
-// r*C + 8*cg + c in row m = c*16 + r.
-// Dynamic shared memory (1024-aligned): A 16 KB, B 8 KB, transpose 16x128 words.
+// grid (ctas, prime groups); block 128.  CTA (x, pg) converts the tiles
+// x, x + ctas, ... for the 16 primes of group pg.  Tile index -> (product z,
+// polynomial, column group cg); the tile holds coefficient r*C + Gc*cg + c in
+// row m = r*Gc + c.  A tiles arrive by TMA (box: 128 bytes x Gc columns x R
+// rows, 128-byte swizzle, bytes past the coefficient width zero-filled),
+// double-buffered so the next tile loads while this one is converted.
+// Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose 16x128 words.
 // ---------------------------------------------------------------------------
 template <int LOGR>
-__global__ void __launch_bounds__(128) k1t_convert_cols(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
+__global__ void __launch_bounds__(128) k1t_convert_cols(const __grid_constant__ CUtensorMap map_a,
+                                                        const __grid_constant__ CUtensorMap map_b,
                                                         uint32_t* __restrict__ res,
                                                         const PrimeConst* __restrict__ pcs,
                                                         const uint8_t* __restrict__ conv_w,
                                                         const uint2* __restrict__ tw_fwd, int n, int logC, int P,
-                                                        int stride_bytes, int count, size_t io_bstride_bytes,
-                                                        size_t ws_bstride, uint32_t* __restrict__ err) {
+                                                        int count, size_t ws_bstride, uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sA = sbase;                        // 128 x 128 B
-    uint8_t* sB = sbase + 16384;                // 64 x 128 B
-    uint32_t* sT = reinterpret_cast<uint32_t*>(sbase + 16384 + 8192);  // [16][128] residues
-    __shared__ uint64_t bar;
+    uint8_t* sA = sbase;                        // 2 x (128 x 128 B)
+    uint8_t* sB = sbase + 32768;                // 64 x 128 B
+    uint32_t* sT = reinterpret_cast<uint32_t*>(sbase + 32768 + 8192);  // [16][128] residues
+    __shared__ uint64_t tma_bar[2], mma_bar;
     __shared__ uint32_t tmem_base;
     __shared__ PrimeConst spc[tc::kConvGroup];
 
@@ -170,22 +190,36 @@ __global__ void __launch_bounds__(128) k1t_convert_cols(const uint8_t* __restric
     const int tiles = count * 2 * groups_per_poly;
     const int np = min(tc::kConvGroup, P - pg * tc::kConvGroup);  // primes in this group
 
-    // B operand: this group's pre-swizzled weight image; A: zero once (bytes past
-    // the coefficient width stay zero for every tile)
+    // B: this group's pre-swizzled weight image.  A: zero once -- rows past
+    // R*Gc (small rings) are never written by the TMA and must stay zero.
     {
         const uint4* src = reinterpret_cast<const uint4*>(conv_w + size_t(pg) * 8192);
         for (int k = tid; k < 512; k += 128) reinterpret_cast<uint4*>(sB)[k] = __ldg(src + k);
-        for (int k = tid; k < 1024; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
+        for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
         if (tid < tc::kConvGroup) spc[tid] = pcs[min(pg * tc::kConvGroup + tid, P - 1)];
     }
     if (warp == 0) tc::tmem_alloc(&tmem_base, 64);
-    if (tid == 0) tc::mbar_init(&bar, 1);
+    if (tid == 0) {
+        tc::mbar_init(&tma_bar[0], 1);
+        tc::mbar_init(&tma_bar[1], 1);
+        tc::mbar_init(&mma_bar, 1);
+    }
     tc::fence_smem_async();
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     const uint32_t tbase = tmem_base;
     const uint32_t taddr = tbase + (uint32_t(32 * (warp & 3)) << 16);
+    const uint32_t tile_bytes = 128u * uint32_t(Gc) * uint32_t(R);
+
+    auto issue = [&](int tile, int buf) {
+        const int cg = tile % groups_per_poly;
+        const int poly = (tile / groups_per_poly) & 1;
+        const int z = tile / (2 * groups_per_poly);
+        tc::mbar_expect_tx(&tma_bar[buf], tile_bytes);
+        tc::tma_load_4d(sA + buf * 16384, poly ? &map_b : &map_a, 0, cg * Gc, 0, z, &tma_bar[buf]);
+    };
+    if (tid == 0 && int(blockIdx.x) < tiles) issue(blockIdx.x, 0);
 
     // column-stage role: prime j of the group, column c of the tile
     const int cj = tid / 8, cc = tid % 8;
@@ -196,38 +230,29 @@ __global__ void __launch_bounds__(128) k1t_convert_cols(const uint8_t* __restric
     for (int k = 1; k < R; ++k) twr[k - 1] = __ldg(tw_fwd + size_t(ci) * kNMax + k);
     const PrimeConst cpc = pcs[ci];
 
-    uint32_t phase = 0;
+    uint32_t tma_phases = 0, mma_phase = 0;  // bit b: parity of buffer b's next TMA completion
     bool ok = true;
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    int k = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+        const int buf = k & 1;
         const int cg = tile % groups_per_poly;
         const int poly = (tile / groups_per_poly) & 1;
         const int z = tile / (2 * groups_per_poly);
-        // --- stage the tile's coefficient bytes into A (8-byte pieces) ---
-        const uint8_t* src = (poly ? b : a) + size_t(z) * io_bstride_bytes;
-        const int seg = Gc * stride_bytes;  // bytes of one row's Gc coefficients (contiguous)
-        for (int p = tid * 8; p < R * seg; p += 128 * 8) {
-            const int r = p / seg, off = p - r * seg;
-            const int c = off / stride_bytes, kb = off - c * stride_bytes;
-            if (kb < 128) {
-                const uint2 v = __ldg(reinterpret_cast<const uint2*>(
-                    src + (size_t(r) * C + size_t(cg) * Gc + c) * stride_bytes + kb));
-                *reinterpret_cast<uint2*>(sA + tc::sw128_offset(c * R + r, kb)) = v;
-            }
-        }
-        tc::fence_smem_async();
-        tc::fence_before();
-        __syncthreads();
         if (tid == 0) {
+            ok = tc::mbar_wait(&tma_bar[buf], (tma_phases >> buf) & 1u) && ok;
             tc::fence_after();
-            const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+            const uint32_t a0 = tc::smem_u32(sA + buf * 16384), b0 = tc::smem_u32(sB);
             constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kConvN);
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks)
                 tc::mma_u8(tbase, tc::sw128_desc(a0 + 32 * ks), tc::sw128_desc(b0 + 32 * ks), idesc, ks > 0);
-            tc::mma_commit(&bar);
+            tc::mma_commit(&mma_bar);
+            // the other buffer's last reader was the previous tile's MMA, already complete
+            if (tile + int(gridDim.x) < tiles) issue(tile + gridDim.x, buf ^ 1);
         }
-        ok = tc::mbar_wait(&bar, phase) && ok;
-        phase ^= 1;
+        tma_phases ^= 1u << buf;
+        ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
+        mma_phase ^= 1;
         tc::fence_after();
         // --- residues of row m = tid for the group's 16 primes ---
 #pragma unroll
@@ -249,7 +274,7 @@ __global__ void __launch_bounds__(128) k1t_convert_cols(const uint8_t* __restric
         if (col_active) {
             uint32_t v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = sT[cj * 128 + cc * R + r];
+            for (int r = 0; r < R; ++r) v[r] = sT[cj * 128 + r * Gc + cc];
 #pragma unroll
             for (int s = 0; s < LOGR; ++s) {
                 const int t = R >> (s + 1);
@@ -261,6 +286,7 @@ __global__ void __launch_bounds__(128) k1t_convert_cols(const uint8_t* __restric
 #pragma unroll
             for (int r = 0; r < R; ++r) dst[size_t(r) << logC] = v[r];
         }
+        __syncthreads();  // sT is rewritten by the next tile
     }
     tc::fence_before();
     __syncthreads();
@@ -273,26 +299,31 @@ __global__ void __launch_bounds__(128) k1t_convert_cols(const uint8_t* __restric
 
 // ---------------------------------------------------------------------------
 // K3T: inverse column stages + CRT on the tensor cores.
-// grid (ctas); block 128.  Tile index -> (product z, column group cg).
-// Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB.
+// grid (ctas); block 128.  Tile index -> (product z, column group cg).  The
+// tile's residues for every prime arrive by TMA (box: Gc columns x R rows x P
+// primes of u32); the next tile's box is requested as soon as this one has
+// been turned into CRT digits, so it loads during the MMA and the epilogue.
+// Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB,
+// residue box P*R*Gc words, inverse column twiddles P*(R-1) uint2.
 // ---------------------------------------------------------------------------
 template <int LOGR, int W>
-__global__ void __launch_bounds__(128) k3t_cols_crt(const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
-                                                    const PrimeConst* __restrict__ pcs,
+__global__ void __launch_bounds__(128) k3t_cols_crt(const __grid_constant__ CUtensorMap map_res,
+                                                    uint32_t* __restrict__ out, const PrimeConst* __restrict__ pcs,
                                                     const uint2* __restrict__ tw_inv,
                                                     const uint2* __restrict__ scale,
                                                     const uint8_t* __restrict__ crt_w,
                                                     const uint32_t* __restrict__ consts, uint64_t mu_q, int sbits,
                                                     int n, int logC, int P, int stride, int count,
-                                                    size_t io_bstride, size_t ws_bstride,
-                                                    uint32_t* __restrict__ err) {
+                                                    size_t io_bstride, const uint32_t* __restrict__ work,
+                                                    size_t ws_bstride, int use_tma, uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
     constexpr int NV = 4 * W + 4;  // value byte columns
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = sbase;          // [2][128][128 B]
     uint8_t* sB = sbase + 32768;  // [2][128][128 B]
-    __shared__ uint64_t bar;
+    uint32_t* sR = reinterpret_cast<uint32_t*>(sbase + 65536);  // [P][R][Gc]
+    __shared__ uint64_t tma_bar, mma_bar;
     __shared__ uint32_t tmem_base;
     __shared__ uint32_t s_q[2 * W];
 
@@ -301,14 +332,22 @@ __global__ void __launch_bounds__(128) k3t_cols_crt(const uint32_t* __restrict__
     const int Gc = C < 8 ? C : 8;
     const int groups = C / Gc;
     const int tiles = count * groups;
+    const int box_words = P * R * Gc;
+    uint2* sTw = reinterpret_cast<uint2*>(sR + ((box_words + 3) & ~3));  // [P][R-1]
     {
         const uint4* src = reinterpret_cast<const uint4*>(crt_w);
         for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sB)[k] = __ldg(src + k);
         for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
         for (int k = tid; k < 2 * W; k += 128) s_q[k] = consts[k];
+        constexpr int RT = R > 1 ? R - 1 : 1;
+        if (R > 1)
+            for (int k = tid; k < P * RT; k += 128) sTw[k] = __ldg(tw_inv + size_t(k / RT) * kNMax + 1 + k % RT);
     }
     if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
-    if (tid == 0) tc::mbar_init(&bar, 1);
+    if (tid == 0) {
+        tc::mbar_init(&tma_bar, 1);
+        tc::mbar_init(&mma_bar, 1);
+    }
     tc::fence_smem_async();
     tc::fence_before();
     __syncthreads();
@@ -316,27 +355,44 @@ __global__ void __launch_bounds__(128) k3t_cols_crt(const uint32_t* __restrict__
     const uint32_t tbase = tmem_base;
     const uint32_t taddr = tbase + (uint32_t(32 * (warp & 3)) << 16);
     const int pairs = P * Gc;
+    // rings with fewer than 4 columns (n < 64) have rows too short for a tensor
+    // map; their single-tile box is read by the threads instead
+    auto issue = [&](int tile) {
+        if (!use_tma) return;
+        tc::mbar_expect_tx(&tma_bar, uint32_t(box_words) * 4u);
+        tc::tma_load_4d(sR, &map_res, (tile % groups) * Gc, 0, 0, tile / groups, &tma_bar);
+    };
+    if (tid == 0 && int(blockIdx.x) < tiles) issue(blockIdx.x);
 
-    uint32_t phase = 0;
+    uint32_t tma_phase = 0, mma_phase = 0;
     bool ok = true;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int cg = tile % groups, z = tile / groups;
-        const uint32_t* plane = res + size_t(z) * ws_bstride;
+        if (use_tma) {
+            ok = tc::mbar_wait(&tma_bar, tma_phase) && ok;
+            tma_phase ^= 1;
+        } else {
+            const uint32_t* plane = work + size_t(z) * ws_bstride;
+            for (int k = tid; k < box_words; k += 128) {
+                const int c = k % Gc, r = (k / Gc) % R, i = k / (Gc * R);
+                sR[k] = plane[size_t(i) * n + (size_t(r) << logC) + size_t(cg) * Gc + c];
+            }
+            __syncthreads();
+        }
         // --- inverse column stages and CRT digits into A ---
         for (int pr = tid; pr < pairs; pr += 128) {
             const int i = pr / Gc, c = pr - i * Gc;
             const PrimeConst pc = pcs[i];
-            const uint32_t* srcp = plane + size_t(i) * n + size_t(cg) * Gc + c;
             uint32_t v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = srcp[size_t(r) << logC];
-            const uint2* tw = tw_inv + size_t(i) * kNMax;
+            for (int r = 0; r < R; ++r) v[r] = sR[(i * R + r) * Gc + c];
+            const uint2* tw = sTw + i * (R - 1) - 1;  // tw[k] = Psi_inv_rev[k], k >= 1
 #pragma unroll
             for (int s = LOGR - 1; s >= 0; --s) {
                 const int t = R >> (s + 1);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (!(r & t)) gs_bfly(v[r], v[r + t], __ldg(tw + (1 << s) + (r >> (LOGR - s))), pc.p, pc.two_p);
+                    if (!(r & t)) gs_bfly(v[r], v[r + t], tw[(1 << s) + (r >> (LOGR - s))], pc.p, pc.two_p);
             }
             const uint2 sc = __ldg(scale + i);
             const uint32_t ka = uint32_t(i) >> 5, kb = (4u * i) & 127u;
@@ -351,6 +407,8 @@ __global__ void __launch_bounds__(128) k3t_cols_crt(const uint32_t* __restrict__
         __syncthreads();
         if (tid == 0) {
             tc::fence_after();
+            // the residue box is free again: fetch the next tile's during the MMA and epilogue
+            if (tile + int(gridDim.x) < tiles) issue(tile + gridDim.x);
             const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
             constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kCrtN);
 #pragma unroll
@@ -358,10 +416,10 @@ __global__ void __launch_bounds__(128) k3t_cols_crt(const uint32_t* __restrict__
                 const uint32_t off = (ks >> 2) * 16384 + 32 * (ks & 3);
                 tc::mma_u8(tbase, tc::sw128_desc(a0 + off), tc::sw128_desc(b0 + off), idesc, ks > 0);
             }
-            tc::mma_commit(&bar);
+            tc::mma_commit(&mma_bar);
         }
-        ok = tc::mbar_wait(&bar, phase) && ok;
-        phase ^= 1;
+        ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
+        mma_phase ^= 1;
         tc::fence_after();
         // --- carry-propagate the byte columns of row m = tid ---
         // value: NV/4 = W+1 words plus the carry-out; quotient estimate: 8 columns
@@ -391,9 +449,8 @@ __global__ void __launch_bounds__(128) k3t_cols_crt(const uint32_t* __restrict__
         }
         acc[W + 1] = uint32_t(carry);
         const uint64_t f1 = fsum1 + (fsum0 >> 32);
-        const uint32_t fr[3] = {uint32_t(fsum0), uint32_t(f1), uint32_t(f1 >> 32)};
-        // nearest integer of sum t_i / p_i: F = fr[2]:fr[1]:fr[0] / 2^64, rounded
-        const uint32_t nearest = fr[2] + (fr[1] >> 31);
+        // nearest integer of sum t_i / p_i: (f1 * 2^32 + low) / 2^64 rounded
+        const uint32_t nearest = uint32_t(f1 >> 32) + (uint32_t(f1) >> 31);
         const int cc = tid / R, rr = tid % R;
         if (cc < Gc) {
             const size_t J = (size_t(rr) << logC) + size_t(cg) * Gc + cc;
@@ -435,7 +492,7 @@ std::vector<uint8_t> conversion_image(const std::vector<uint32_t>& primes) {
 void tensor_init(PlanCore& s) {
     if (uint32_t(s.P) * 4 > uint32_t(tc::kCrtK)) throw Failure(PM_ERR_UNSUPPORTED, "prime basis too large for the CRT tile");
     if (4 * s.W + 4 + 8 > uint32_t(tc::kCrtN)) throw Failure(PM_ERR_UNSUPPORTED, "q too wide for the CRT tile");
-    if (s.stride % 2) throw Failure(PM_ERR_UNSUPPORTED, "tensor path needs whole u64 limbs");
+    if (s.stride % 4) throw Failure(PM_ERR_UNSUPPORTED, "tensor path needs an even coef_limbs (16-byte coefficient rows)");
     DeviceBasis& B = *s.basis;
     {
         static std::mutex m;
@@ -493,38 +550,88 @@ int sm_count() {
     return count;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cuda_check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q),
+                   "look up cuTensorMapEncodeTiled");
+        if (!p || q != cudaDriverEntryPointSuccess) throw Failure(PM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 4-D map with packed (nested) strides; dims[0] contiguous.
+CUtensorMap make_map(CUtensorMapDataType type, const void* base, const cuuint64_t dims[4],
+                     const cuuint64_t strides_bytes[3], const cuuint32_t box[4], CUtensorMapSwizzle swizzle) {
+    CUtensorMap map;
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    const CUresult r = encode_fn()(&map, type, 4, const_cast<void*>(base), dims, strides_bytes, box, estride,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Failure(PM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return map;
+}
+
+// coefficient bytes of `count` products: dims (byte, column, row, product)
+CUtensorMap coefficient_map(const PlanCore& s, const void* base, uint32_t count) {
+    const uint32_t C = 1u << s.logC, R = 1u << s.logR, Gc = C < 8 ? C : 8;
+    const cuuint64_t sb = s.stride * 4ull;
+    const cuuint64_t dims[4] = {sb, C, R, count};
+    const cuuint64_t strides[3] = {sb, sb * C, sb * C * R};
+    const cuuint32_t box[4] = {128, Gc, R, 1};
+    return make_map(CU_TENSOR_MAP_DATA_TYPE_UINT8, base, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+// the product planes (plane 0..P-1) of `count` workspaces: dims (column, row, prime, product)
+CUtensorMap residue_map(const PlanCore& s, const void* work, uint32_t count) {
+    const uint32_t C = 1u << s.logC, R = 1u << s.logR, Gc = C < 8 ? C : 8;
+    const cuuint64_t dims[4] = {C, R, s.P, count};
+    const cuuint64_t strides[3] = {C * 4ull, C * R * 4ull, s.workspace_bytes};
+    const cuuint32_t box[4] = {Gc, R, s.P, 1};
+    return make_map(CU_TENSOR_MAP_DATA_TYPE_UINT32, work, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE);
+}
+
 template <int LOGR>
 void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, uint32_t count,
                 cudaStream_t st) {
     const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
     const int groups = int((s.P + tc::kConvGroup - 1) / tc::kConvGroup);
     const int tiles = int(count) * 2 * (C / Gc);
-    int ctas = sm_count() * 6 / groups;
+    int ctas = sm_count() * 4 / groups;
     if (ctas > tiles) ctas = tiles;
     if (ctas < 1) ctas = 1;
-    const size_t smem = 1024 + 16384 + 8192 + 16 * 128 * 4;
+    const size_t smem = 1024 + 32768 + 8192 + 16 * 128 * 4;
     cuda_check(cudaFuncSetAttribute(k1t_convert_cols<LOGR>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K1T shared memory");
+    const CUtensorMap ma = coefficient_map(s, a, count), mb = coefficient_map(s, b, count);
     dim3 grid(ctas, groups);
-    k1t_convert_cols<LOGR><<<grid, 128, smem, st>>>(
-        reinterpret_cast<const uint8_t*>(a), reinterpret_cast<const uint8_t*>(b), work, s.basis->d_pc,
-        s.basis->d_conv_weights, s.basis->d_tw_fwd, int(s.n), int(s.logC), int(s.P), int(s.stride * 4),
-        int(count), size_t(s.n) * s.stride * 4, s.workspace_bytes / 4, s.d_err);
+    k1t_convert_cols<LOGR><<<grid, 128, smem, st>>>(ma, mb, work, s.basis->d_pc, s.basis->d_conv_weights,
+                                                    s.basis->d_tw_fwd, int(s.n), int(s.logC), int(s.P), int(count),
+                                                    s.workspace_bytes / 4, s.d_err);
 }
 
 template <int LOGR, int W>
 void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t count, cudaStream_t st) {
-    const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
+    const int C = 1 << s.logC, Gc = C < 8 ? C : 8, R = 1 << s.logR;
     const int tiles = int(count) * (C / Gc);
-    int ctas = sm_count() * 3;
+    int ctas = sm_count() * 2;
     if (ctas > tiles) ctas = tiles;
-    const size_t smem = 1024 + 65536;
+    const size_t box_words = size_t(s.P) * R * Gc;
+    const size_t smem = 1024 + 65536 + ((box_words + 3) & ~size_t(3)) * 4 + size_t(s.P) * (R > 1 ? R - 1 : 1) * 8;
     cuda_check(cudaFuncSetAttribute(k3t_cols_crt<LOGR, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K3T shared memory");
-    k3t_cols_crt<LOGR, W><<<ctas, 128, smem, st>>>(work, c, s.basis->d_pc, s.basis->d_tw_inv, s.d_scale,
+    const bool use_tma = (C * 4) % 16 == 0;
+    CUtensorMap mr;
+    std::memset(&mr, 0, sizeof mr);
+    if (use_tma) mr = residue_map(s, work, count);
+    k3t_cols_crt<LOGR, W><<<ctas, 128, smem, st>>>(mr, c, s.basis->d_pc, s.basis->d_tw_inv, s.d_scale,
                                                     s.d_crt_weights, s.d_consts, s.mu_q, int(s.qbits), int(s.n),
                                                     int(s.logC), int(s.P), int(s.stride), int(count),
-                                                    size_t(s.n) * s.stride, s.workspace_bytes / 4, s.d_err);
+                                                    size_t(s.n) * s.stride, work, s.workspace_bytes / 4,
+                                                    use_tma ? 1 : 0, s.d_err);
 }
 
 template <int LOGR>

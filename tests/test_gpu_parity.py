@@ -26,6 +26,12 @@ def make_plan(path, n, q, limbs=None):
     return polymul.Plan(n, q, coef_limbs=limbs, tensor=(path == "tensor"))
 
 
+def limbs_for(path, bits):
+    """u64 limbs per coefficient: the tensor path reads 16-byte coefficient rows."""
+    limbs = (bits + 63) // 64
+    return limbs + (limbs % 2) if path == "tensor" else limbs
+
+
 def test_golden_points(cuda, golden, path):
     for point in golden["points"]:
         q = int(point["q"], 16)
@@ -49,8 +55,9 @@ def test_widths(cuda, path, bits):
     n = 1024
     rng = np.random.default_rng(bits)
     q = random_q(rng, bits)
-    a, b = uniform_below(rng, q, n), uniform_below(rng, q, n)
-    with make_plan(path, n, q) as p:
+    limbs = limbs_for(path, bits)
+    a, b = uniform_below(rng, q, n, limbs), uniform_below(rng, q, n, limbs)
+    with make_plan(path, n, q, limbs) as p:
         assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
 
 
@@ -120,7 +127,7 @@ def test_batch_api(cuda, path, n, bits, count):
     torch = cuda
     rng = np.random.default_rng(n + count)
     q = random_q(rng, bits)
-    limbs = (bits + 63) // 64
+    limbs = limbs_for(path, bits)
     a = np.stack([uniform_below(rng, q, n, limbs) for _ in range(count)])
     b = np.stack([uniform_below(rng, q, n, limbs) for _ in range(count)])
     with make_plan(path, n, q, limbs) as p:
@@ -164,3 +171,9 @@ def test_paths_agree_bitwise(cuda):
     a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
     with make_plan("simt", n, q, 14) as p1, make_plan("tensor", n, q, 14) as p2:
         assert (p1.multiply_host(a, b) == p2.multiply_host(a, b)).all()
+
+
+def test_tensor_path_refuses_odd_limbs(cuda):
+    with pytest.raises(polymul.PolymulError) as e:
+        make_plan("tensor", 1024, random_q(np.random.default_rng(1), 517), 9)
+    assert e.value.status == polymul.PM_ERR_UNSUPPORTED
