@@ -101,3 +101,8 @@ void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint
                    uint32_t count, cudaStream_t st);
 
 }  // namespace pm
+
+// The C ABI's opaque plan handle.
+struct pm_plan {
+    pm::PlanCore core;
+};

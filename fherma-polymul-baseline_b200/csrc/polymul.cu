@@ -552,10 +552,6 @@ void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* 
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
-struct pm_plan {
-    pm::PlanCore core;
-};
-
 using pm::fail;
 using pm::Failure;
 

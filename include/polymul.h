@@ -103,6 +103,20 @@ int pm_batch_workspace_size(const pm_plan* plan, uint32_t count, size_t* bytes);
 int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c);
 
 /*
+ * One product, like pm_multiply, but the call allocates nothing: no
+ * cudaMalloc, no cudaFree, no allocating library routine.  Its residue
+ * scratch is a 4 MiB array built into the library (one per GPU), so it serves
+ * plans whose workspace_bytes fit in 4 MiB (n <= 8192 for an 868-bit q) and
+ * refuses larger ones with PM_ERR_UNSUPPORTED.  For callers that cannot
+ * allocate device memory when they multiply.  All calls on a device share the
+ * array: calls that overlap on the GPU race.  The first call on each device
+ * looks the array's address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  This entry point has no counterpart in the
+ * reference, which always multiplies in buffers it allocated in fherma_init.
+ */
+int pm_multiply_noalloc(const pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, pm_stream stream);
+
+/*
  * Host-only (no GPU needed): the RNS basis a plan for (n, q_bits) would use.
  * Writes up to `capacity` primes (descending, p = 1 mod 2^17, p < 2^30) and
  * sets *count.  Mirrors rns::setup's prime search (rns/host_setup.h:67-83).
