@@ -44,13 +44,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=32768)
+    ap.add_argument("--ring", type=int, default=32768, help="ring dimension N")
     ap.add_argument("--bits", type=int, default=868)
     ap.add_argument("--batch", type=int, default=512, help="independent products per step")
     ap.add_argument("--e2e-batch", type=int, default=16)
-    ap.add_argument("--tensor", action="store_true", help="tcgen05 INT8 conversion/CRT")
+    ap.add_argument("--path", default="tensor", choices=["tensor", "simt"],
+                    help="tensor: tcgen05 INT8 conversion/CRT (default); simt: the plain CUDA-core method")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ncu-case", type=int, default=0, metavar="K",
+                    help="no timing: run K single products (one launch sequence each) for an ncu capture")
     return ap.parse_args()
 
 
@@ -73,6 +76,17 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def max_over_ranks(value, dist, world, device):
+    """The slowest rank's time: every rank contributes, every rank gets the max."""
+    if world <= 1:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def init_dist(world, backend):
@@ -118,7 +132,7 @@ def run_reference(args):
         return
     threads = os.cpu_count() or 1
     q = seeded_q(args.seed, args.bits)
-    (a, b), = host_inputs(args.n, q, args.seed + 1)
+    (a, b), = host_inputs(args.ring, q, args.seed + 1)
     from oracle import oracle
 
     for _ in range(max(args.warmup, 1)):
@@ -132,11 +146,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"one negacyclic product per step, N={args.n}, {args.bits}-bit seeded odd q, "
-                               "coefficients uniform in [0, q)", "n": args.n, "q_bits": args.bits,
+        "config": {"workload": f"one negacyclic product per step, N={args.ring}, {args.bits}-bit seeded odd q, "
+                               "coefficients uniform in [0, q)", "n": args.ring, "q_bits": args.bits,
                    "parallelism": "cpu threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} products at N={args.n}; the reference's RNS method restated in C "
+                         "sample": f"{args.steps} products at N={args.ring}; the reference's RNS method restated in C "
                                    "(oracle/polymul_oracle.c), threads over primes; the reference's own path "
                                    "needs cuPQC and a GPU"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -275,10 +289,10 @@ def run_ours(args):
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
     dist = init_dist(world, "nccl")
-    n, bits = args.n, args.bits
+    n, bits = args.ring, args.bits
     q = seeded_q(args.seed, bits)
     limbs = (bits + 63) // 64
-    plan = polymul.Plan(n, q, coef_limbs=limbs, tensor=args.tensor)
+    plan = polymul.Plan(n, q, coef_limbs=limbs, tensor=(args.path == "tensor"))
     B = args.batch
     A = device_inputs(torch, B, n, limbs, q, args.seed + 17 + 1000 * rank)
     Bv = device_inputs(torch, B, n, limbs, q, args.seed + 29 + 1000 * rank)
@@ -331,11 +345,7 @@ def run_ours(args):
     launches = polymul.launch_count() - launches0
     prof = polymul.profile_read()
     polymul.profile_enable(0)
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, world, "cuda")
     total_products = B * args.steps * world
     value = total_products / (ms / 1000.0)
 
@@ -363,11 +373,7 @@ def run_ours(args):
     for _ in range(args.steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, world, "cuda")
     e2e_value = E * args.steps * world / e2e_s
     io = n * 8 * limbs
 
@@ -417,7 +423,7 @@ def run_ours(args):
             "config": {"workload": f"batch of {B} independent negacyclic products per step, N={n}, {bits}-bit "
                                    f"seeded odd q, coefficients uniform in [0, q) generated on the device",
                        "n": n, "q_bits": bits, "batch": B, "primes": plan.primes,
-                       "path": "tensor" if args.tensor else "simt",
+                       "path": args.path,
                        "l2": f"inputs larger than L2: {2 * B * io / 1e9:.2f} GB of a, b read per step",
                        "parallelism": f"replicas x{world}", "oracle_check": f"{checked} products bit-exact"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * E * io, "d2h_bytes_per_step": E * io,
@@ -436,8 +442,31 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_ncu_case(args):
+    """K single products of the benchmark workload, for `ncu -k ... -s ... -c ...` captures."""
+    import torch
+
+    import polymul
+
+    torch.cuda.set_device(0)
+    q = seeded_q(args.seed, args.bits)
+    limbs = (args.bits + 63) // 64
+    a = device_inputs(torch, args.ncu_case, args.ring, limbs, q, args.seed + 17)
+    b = device_inputs(torch, args.ncu_case, args.ring, limbs, q, args.seed + 29)
+    c = torch.empty_like(a)
+    plan = polymul.Plan(args.ring, q, coef_limbs=limbs, tensor=(args.path == "tensor"))
+    for k in range(args.ncu_case):
+        plan.multiply(a[k].data_ptr(), b[k].data_ptr(), c[k].data_ptr())
+    torch.cuda.synchronize()
+    plan.close()
+    print(f"ncu case: {args.ncu_case} products, N={args.ring}, {args.bits}-bit q, path {args.path}")
+
+
 def main():
     args = parse()
+    if args.ncu_case:
+        run_ncu_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         world, _, _ = dist_env()

@@ -1,0 +1,67 @@
+// fherma_init / fherma_run / fherma_free on top of the C ABI (include/polymul.h).
+// Status codes become std::runtime_error, as the reference's check() does
+// (rns/solve.cu:421-423).
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/fherma_polymul.h"
+#include "../../include/polymul.h"
+
+namespace {
+
+struct State {
+    pm_plan* plan = nullptr;
+    uint32_t n = 0, words = 0;
+    ~State() { pm_plan_destroy(plan); }
+};
+
+[[noreturn]] void raise(int status, const char* what) {
+    throw std::runtime_error(std::string(what) + ": " + pm_status_string(status) + " (" + pm_last_error() + ")");
+}
+
+unsigned bit_length(const std::vector<uint32_t>& w) {
+    for (size_t i = w.size(); i--;)
+        if (w[i]) return unsigned(i * 32 + 32 - __builtin_clz(w[i]));
+    return 0;
+}
+
+}  // namespace
+
+void* fherma_init(const fherma::Point& p) {
+    if (p.L == 0 || p.q.data.size() != p.L) throw std::runtime_error("fherma_init: q must hold L words");
+    if (p.L % 2) throw std::runtime_error("fherma_init: L must be even (coefficients are read as 64-bit limbs)");
+    if (p.N < 2 || (p.N & (p.N - 1)) || p.N > 65536)
+        throw std::runtime_error("fherma_init: N must be a power of two in [2, 65536]");
+    const unsigned bits = bit_length(p.q.data);
+    if (p.W && bits > p.W) throw std::runtime_error("fherma_init: q is wider than W bits");
+    std::vector<uint64_t> q64(p.L / 2);
+    for (uint32_t i = 0; i < p.L / 2; ++i) q64[i] = uint64_t(p.q.data[2 * i]) | (uint64_t(p.q.data[2 * i + 1]) << 32);
+    auto s = std::make_unique<State>();
+    s->n = p.N;
+    s->words = p.L;
+    const uint32_t limbs = p.L / 2;
+    // the tensor-core conversion reads 16-byte coefficient rows (even limb counts)
+    const uint32_t flags = (limbs % 2 == 0) ? PM_CONVERT_TENSOR : PM_CONVERT_SIMT;
+    const int st = pm_plan_create(&s->plan, p.N, q64.data(), limbs, limbs, flags);
+    if (st != PM_OK) raise(st, "fherma_init");
+    return s.release();
+}
+
+fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
+    if (!state) throw std::runtime_error("fherma_run: no state");
+    auto& s = *static_cast<State*>(state);
+    const size_t words = size_t(s.n) * s.words;
+    if (in.a.data.size() != words || in.b.data.size() != words)
+        throw std::runtime_error("fherma_run: inputs must be N x L words");
+    fherma::Outputs out;
+    out.c.shape = {int64_t(s.n), int64_t(s.words)};
+    out.c.data.resize(words);
+    const int st = pm_multiply_host(s.plan, reinterpret_cast<const uint64_t*>(in.a.data.data()),
+                                    reinterpret_cast<const uint64_t*>(in.b.data.data()),
+                                    reinterpret_cast<uint64_t*>(out.c.data.data()));
+    if (st != PM_OK) raise(st, "fherma_run");
+    return out;
+}
+
+void fherma_free(void* state) { delete static_cast<State*>(state); }
