@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -50,6 +51,17 @@ DeviceBasis& basis_for_device(int device);
 std::vector<uint32_t> make_primes();
 unsigned basis_size(const std::vector<uint32_t>& primes, unsigned n, unsigned qbits);
 
+// One stage of the host-batch pipeline: a stream with its own device buffers
+// (a, b, c and the residue workspace of a group) and pinned staging.
+struct PipelineSlot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    void* d_buf = nullptr;
+    void* h_buf = nullptr;
+    bool pending = false;
+    ~PipelineSlot();
+};
+
 // Everything one (n, q) product needs on the device.
 struct PlanCore {
     int device = 0;
@@ -78,8 +90,12 @@ struct PlanCore {
     uint32_t* d_err = nullptr;     // set by a kernel whose bounded wait ran out
     uint32_t tensor_k_crt = 0;
 
+    std::unique_ptr<PipelineSlot> pipe[3];
+    uint32_t pipe_group = 0;
+
     void init(uint32_t n, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs, uint32_t flags);
     void ensure_batch_workspace(uint32_t group);
+    void ensure_pipeline(uint32_t group);
     ~PlanCore();
 };
 
@@ -93,6 +109,7 @@ void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint6
 void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                     cudaStream_t st);
 void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c);
+void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count);
 
 // tensor-core conversion / CRT (tensor.cu)
 void tensor_init(PlanCore& s);

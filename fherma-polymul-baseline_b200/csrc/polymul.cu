@@ -255,6 +255,7 @@ PlanCore::~PlanCore() {
     cudaFree(d_mq);
     cudaFree(d_consts);
     cudaFree(d_scale);
+    for (auto& sl : pipe) sl.reset();
     tensor_release(*this);
     cudaFree(d_work);
     cudaFree(d_batch_work);
@@ -547,6 +548,105 @@ void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* 
     if (!pc) std::memcpy(c, stage + 2 * s.io_bytes, s.io_bytes);
 }
 
+// ---------------------------------------------------------------------------
+// host batches: chunks of `group` products rotate over three slots, each with
+// its own stream, device buffers and workspace, so one slot's H2D, another's
+// kernels and a third's D2H run at the same time.  Pageable buffers are staged
+// through the slot's pinned memory by the calling thread.
+// ---------------------------------------------------------------------------
+PipelineSlot::~PipelineSlot() {
+    if (stream) cudaStreamSynchronize(stream);
+    cudaFree(d_buf);
+    cudaFreeHost(h_buf);
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void PlanCore::ensure_pipeline(uint32_t group) {
+    if (pipe_group >= group && pipe[0]) return;
+    for (auto& sl : pipe) sl.reset();
+    pipe_group = 0;
+    for (auto& sl : pipe) {
+        sl = std::make_unique<PipelineSlot>();
+        cuda_check(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "pipeline stream");
+        cuda_check(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming), "pipeline event");
+        cuda_check(cudaMalloc(&sl->d_buf, size_t(group) * (3 * io_bytes + workspace_bytes)), "pipeline buffers");
+        cuda_check(cudaMallocHost(&sl->h_buf, size_t(group) * 3 * io_bytes), "pipeline staging");
+        sl->pending = false;
+    }
+    pipe_group = group;
+}
+
+void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count) {
+    if (!count) return;
+    uint32_t g = group_size(s);
+    if (g > count) g = count;
+    s.ensure_pipeline(g);
+    auto pinned = [](const void* p) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    const bool pa = pinned(a), pb = pinned(b), pc = pinned(c);
+    const size_t io = s.io_bytes;
+    struct Out {
+        uint8_t* dst;
+        const uint8_t* staged;
+        size_t bytes;
+    };
+    Out outs[3] = {};
+    const uint8_t* A = reinterpret_cast<const uint8_t*>(a);
+    const uint8_t* B = reinterpret_cast<const uint8_t*>(b);
+    uint8_t* Cc = reinterpret_cast<uint8_t*>(c);
+    uint32_t k = 0;
+    for (uint32_t z = 0; z < count; z += g, ++k) {
+        const uint32_t cnt = count - z < g ? count - z : g;
+        PipelineSlot& sl = *s.pipe[k % 3];
+        const size_t bytes = size_t(cnt) * io;
+        if (sl.pending) {  // the slot's previous chunk must be out before its buffers are reused
+            cuda_check(cudaEventSynchronize(sl.done), "pipeline chunk");
+            Out& o = outs[k % 3];
+            if (o.staged) std::memcpy(o.dst, o.staged, o.bytes);
+            sl.pending = false;
+        }
+        uint8_t* dev = static_cast<uint8_t*>(sl.d_buf);
+        uint8_t* stage = static_cast<uint8_t*>(sl.h_buf);
+        uint8_t *da = dev, *db = dev + size_t(g) * io, *dc = dev + 2 * size_t(g) * io;
+        void* ws = dev + 3 * size_t(g) * io;
+        const void* sa = A + size_t(z) * io;
+        const void* sb = B + size_t(z) * io;
+        if (!pa) {
+            std::memcpy(stage, sa, bytes);
+            sa = stage;
+        }
+        if (!pb) {
+            std::memcpy(stage + size_t(g) * io, sb, bytes);
+            sb = stage + size_t(g) * io;
+        }
+        cuda_check(cudaMemcpyAsync(da, sa, bytes, cudaMemcpyHostToDevice, sl.stream), "batch a to device");
+        cuda_check(cudaMemcpyAsync(db, sb, bytes, cudaMemcpyHostToDevice, sl.stream), "batch b to device");
+        launch_batch(s, reinterpret_cast<const uint64_t*>(da), reinterpret_cast<const uint64_t*>(db),
+                     reinterpret_cast<uint64_t*>(dc), cnt, g, ws, sl.stream);
+        uint8_t* out = Cc + size_t(z) * io;
+        uint8_t* land = pc ? out : stage + 2 * size_t(g) * io;
+        cuda_check(cudaMemcpyAsync(land, dc, bytes, cudaMemcpyDeviceToHost, sl.stream), "batch c to host");
+        cuda_check(cudaEventRecord(sl.done, sl.stream), "pipeline event");
+        outs[k % 3] = Out{out, pc ? nullptr : land, bytes};
+        sl.pending = true;
+    }
+    for (int i = 0; i < 3; ++i) {
+        PipelineSlot& sl = *s.pipe[i];
+        if (!sl.pending) continue;
+        cuda_check(cudaEventSynchronize(sl.done), "pipeline drain");
+        if (outs[i].staged) std::memcpy(outs[i].dst, outs[i].staged, outs[i].bytes);
+        sl.pending = false;
+    }
+    check_device_errors(s);
+}
+
 }  // namespace pm
 
 // ---------------------------------------------------------------------------
@@ -630,6 +730,12 @@ extern "C" int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_
         }
         pm::launch_batch(s, a, b, c, count, g, workspace, reinterpret_cast<cudaStream_t>(stream));
     })
+}
+
+extern "C" int pm_multiply_host_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c,
+                                      uint32_t count) {
+    if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
+    PM_GUARD(pm::multiply_host_batch(plan->core, a, b, c, count))
 }
 
 extern "C" int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c) {

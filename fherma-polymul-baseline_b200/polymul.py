@@ -43,6 +43,19 @@ class PlanInfo(ctypes.Structure):
                 ("workspace_bytes", ctypes.c_size_t)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("max_group", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("device_budget_bytes", ctypes.c_size_t)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("groups", ctypes.c_uint64), ("peak_inflight", ctypes.c_uint32), ("peak_group", ctypes.c_uint32),
+                ("arena_bytes", ctypes.c_size_t), ("arena_used", ctypes.c_size_t), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("products_per_s", ctypes.c_double)]
+
+
 def lib():
     """Load libpolymul.so once; raises OSError when it was not built."""
     global _lib
@@ -56,9 +69,17 @@ def lib():
         L.pm_plan_destroy.argtypes = [vp]
         L.pm_multiply.argtypes = [vp, vp, vp, vp, vp, vp]
         L.pm_multiply_host.argtypes = [vp, vp, vp, vp]
+        L.pm_multiply_host_batch.argtypes = [vp, vp, vp, vp, u32]
         L.pm_multiply_batch.argtypes = [vp, vp, vp, vp, u32, vp, ctypes.c_size_t, vp]
         L.pm_batch_workspace_size.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_size_t)]
         L.pm_basis_query.argtypes = [u32, u32, ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
+        L.pm_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerConfig)]
+        L.pm_server_submit.argtypes = [vp, u32, u64p, u32, u32, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+        L.pm_server_wait.argtypes = [vp, ctypes.c_uint64, u32]
+        L.pm_server_drain.argtypes = [vp, u32]
+        L.pm_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.pm_server_reset_stats.argtypes = [vp]
+        L.pm_server_destroy.argtypes = [vp]
         L.pm_status_string.restype = ctypes.c_char_p
         L.pm_status_string.argtypes = [ctypes.c_int]
         L.pm_last_error.restype = ctypes.c_char_p
@@ -161,6 +182,20 @@ class Plan:
         check(lib().pm_multiply_host(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
         return c
 
+    def multiply_host_batch(self, a, b, out=None):
+        """(count, n, limbs) host arrays -> products, pipelined over three streams; synchronous."""
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        if a.shape != b.shape or a.ndim != 3 or a.shape[1:] != (self.n, self.coef_limbs):
+            raise PolymulError(PM_ERR_INVALID, f"expected (count, {self.n}, {self.coef_limbs}) arrays")
+        c = np.empty_like(a) if out is None else out
+        check(lib().pm_multiply_host_batch(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data, a.shape[0]))
+        return c
+
+    def multiply_host_batch_ptr(self, a_ptr, b_ptr, c_ptr, count):
+        """Same on raw host pointers (e.g. pinned torch tensors)."""
+        check(lib().pm_multiply_host_batch(self._h, a_ptr, b_ptr, c_ptr, count))
+
     def multiply_batch(self, a_ptr, b_ptr, c_ptr, count, workspace=0, workspace_bytes=0, stream=0):
         """count products stored back to back on the device (asynchronous)."""
         check(lib().pm_multiply_batch(self._h, a_ptr, b_ptr, c_ptr, count, workspace or None, workspace_bytes,
@@ -174,3 +209,49 @@ class Plan:
     def multiply(self, a_ptr, b_ptr, c_ptr, workspace=0, stream=0):
         """Asynchronous product on device pointers (ints) on a CUDA stream handle."""
         check(lib().pm_multiply(self._h, a_ptr, b_ptr, c_ptr, workspace or None, stream or None))
+
+
+class Server:
+    """Continuous-batching serving loop (pm_server_*): submit host buffers, wait on tickets."""
+
+    def __init__(self, slots=8, max_group=8, tensor=True, device_budget_bytes=0):
+        cfg = ServerConfig(slots, max_group, PM_CONVERT_TENSOR if tensor else PM_CONVERT_SIMT, 0,
+                           device_budget_bytes)
+        self._h = ctypes.c_void_p()
+        check(lib().pm_server_create(ctypes.byref(self._h), ctypes.byref(cfg)))
+        self._q = {}
+
+    def submit_ptr(self, n, q, coef_limbs, a_ptr, b_ptr, c_ptr):
+        """Queue one product on host pointers (keep the buffers alive); returns a ticket."""
+        qa = self._q.get(q)
+        if qa is None:
+            qa = self._q[q] = q_limbs_of(q)
+        t = ctypes.c_uint64(0)
+        check(lib().pm_server_submit(self._h, n, qa.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(qa),
+                                     coef_limbs, a_ptr, b_ptr, c_ptr, ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket, timeout_ms=60000):
+        check(lib().pm_server_wait(self._h, ticket, timeout_ms))
+
+    def drain(self, timeout_ms=600000):
+        check(lib().pm_server_drain(self._h, timeout_ms))
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().pm_server_get_stats(self._h, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        check(lib().pm_server_reset_stats(self._h))
+
+    def close(self):
+        if self._h:
+            lib().pm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

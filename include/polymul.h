@@ -117,11 +117,66 @@ int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64
 int pm_multiply_noalloc(const pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, pm_stream stream);
 
 /*
+ * `count` products on host memory, stored back to back ([count][n][coef_limbs]
+ * u64 each), synchronous.  The batch is cut into groups that rotate over three
+ * streams, so the copies in of one group, the kernels of another and the
+ * copies out of a third overlap.  Pinned buffers are copied directly; pageable
+ * ones are staged through pinned memory by the calling thread.  No counterpart
+ * in the reference (one product per fherma_run).
+ */
+int pm_multiply_host_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count);
+
+/*
  * Host-only (no GPU needed): the RNS basis a plan for (n, q_bits) would use.
  * Writes up to `capacity` primes (descending, p = 1 mod 2^17, p < 2^30) and
  * sets *count.  Mirrors rns::setup's prime search (rns/host_setup.h:67-83).
  */
 int pm_basis_query(uint32_t n, uint32_t q_bits, uint32_t* primes, uint32_t capacity, uint32_t* count);
+
+/* ------------------------------------------------------------------------
+ * Serving: products submitted one by one from host threads, admitted onto the
+ * GPU as stream slots and device memory free up (continuous batching).  No
+ * counterpart in the reference (a single-threaded caller, one product per
+ * fherma_run, main.cpp:173-205).
+ * ------------------------------------------------------------------------ */
+typedef struct pm_server pm_server;
+
+typedef struct {
+    uint32_t slots;              /* groups in flight at once, one stream each, 1..64 */
+    uint32_t max_group;          /* same-plan requests merged into one launch (0 = 8) */
+    uint32_t flags;              /* PM_CONVERT_* for the server's plans */
+    uint32_t reserved;
+    size_t device_budget_bytes;  /* arena for the a, b, c and workspaces of in-flight
+                                    groups (0 = a quarter of the free device memory) */
+} pm_server_config;
+
+typedef struct {
+    uint64_t submitted, completed, failed, groups;
+    uint32_t peak_inflight, peak_group;
+    size_t arena_bytes, arena_used;
+    double p50_us, p99_us, mean_us, max_us;  /* submission-to-completion latency */
+    double products_per_s;                   /* completed / (last completion - first submission) */
+} pm_server_stats;
+
+/* Allocates the device arena once; creates the worker thread and streams. */
+int pm_server_create(pm_server** server, const pm_server_config* config);
+/*
+ * Queue c = a*b mod (X^n+1, q); a, b, c are host buffers of n x coef_limbs u64
+ * that must stay valid until pm_server_wait returns for the ticket.  Pinned
+ * buffers let copies overlap; pageable ones work but serialize the worker.
+ * Plans (tables) are created on first use of an (n, q) and stay resident.
+ * PM_ERR_BUSY if one product needs more than the whole arena.
+ */
+int pm_server_submit(pm_server* server, uint32_t n, const uint64_t* q, uint32_t q_limbs, uint32_t coef_limbs,
+                     const uint64_t* a, const uint64_t* b, uint64_t* c, uint64_t* ticket);
+/* Bounded wait for one ticket: PM_OK, PM_ERR_TIMEOUT, or the request's failure. */
+int pm_server_wait(pm_server* server, uint64_t ticket, uint32_t timeout_ms);
+/* Bounded wait until nothing is queued or in flight. */
+int pm_server_drain(pm_server* server, uint32_t timeout_ms);
+int pm_server_get_stats(pm_server* server, pm_server_stats* stats);
+int pm_server_reset_stats(pm_server* server);
+/* Finishes queued work, then releases the arena, streams and plans. */
+int pm_server_destroy(pm_server* server);
 
 const char* pm_status_string(int status);
 /* Message of the last failure on the calling thread ("" if none). */

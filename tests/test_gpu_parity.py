@@ -177,3 +177,27 @@ def test_tensor_path_refuses_odd_limbs(cuda):
     with pytest.raises(polymul.PolymulError) as e:
         make_plan("tensor", 1024, random_q(np.random.default_rng(1), 517), 9)
     assert e.value.status == polymul.PM_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_batch_pipeline(cuda, path, pinned):
+    """pm_multiply_host_batch: host buffers, groups rotating over three streams."""
+    torch = cuda
+    n, count = 16384, 11
+    rng = np.random.default_rng(31 + int(pinned))
+    q = random_q(rng, 868)
+    a = np.stack([uniform_below(rng, q, n, 14) for _ in range(count)])
+    b = np.stack([uniform_below(rng, q, n, 14) for _ in range(count)])
+    with make_plan(path, n, q, 14) as p:
+        if pinned:
+            ha = torch.from_numpy(a.view(np.int64)).pin_memory()
+            hb = torch.from_numpy(b.view(np.int64)).pin_memory()
+            hc = torch.zeros_like(ha).pin_memory()
+            p.multiply_host_batch_ptr(ha.data_ptr(), hb.data_ptr(), hc.data_ptr(), count)
+            got = hc.numpy().view(np.uint64)
+        else:
+            got = p.multiply_host_batch(a, b)
+        for k in range(count):
+            assert (got[k] == p.multiply_host(a[k], b[k])).all(), k
+    for k in (0, count - 1):
+        assert (got[k] == oracle.rns_multiply(a[k], b[k], q)).all()
