@@ -52,6 +52,10 @@ def parse():
                     help="tensor: tcgen05 INT8 conversion/CRT (default); simt: the plain CUDA-core method")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-requests", type=int, default=10000,
+                    help="requests in the serving stream (0 skips it)")
+    ap.add_argument("--serve-rate", type=float, default=6000.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--uneven", type=int, default=64, help="products in the uneven batch (0 skips it)")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="K",
                     help="no timing: run K single products (one launch sequence each) for an ncu capture")
     return ap.parse_args()
@@ -255,6 +259,150 @@ def device_inputs(torch, batch, n, limbs, q, seed):
     raise RuntimeError("rejection sampling did not converge")
 
 
+def run_uneven(args, torch, polymul):
+    """64 products, N log-uniform over {1024..65536}, widths uniform in 200..868 bits
+    (seed 4), as one autotuned graph; against the same products through per-product
+    plans, one launch sequence after another on one stream."""
+    import numpy as np
+
+    from tests.helpers import uniform_below
+
+    rng = np.random.default_rng(4)
+    K = args.uneven
+    ns = [1024 << int(k) for k in rng.integers(0, 7, size=K)]
+    widths = [int(w) for w in rng.integers(200, 869, size=K)]
+    qs = []
+    for w in widths:
+        q = int(rng.integers(0, 2**62)) | 1
+        while q.bit_length() < w:
+            q = (q << 62) | int(rng.integers(0, 2**62))
+        qs.append((q & ((1 << w) - 1)) | (1 << (w - 1)) | 1)
+    a = [uniform_below(rng, q, n, 14) for q, n in zip(qs, ns)]
+    b = [uniform_below(rng, q, n, 14) for q, n in zip(qs, ns)]
+    batch = polymul.Batch(ns, qs, coef_limbs=14)
+    pa, pb = batch.pack(a), batch.pack(b)
+    batch.copy_in(pa.ctypes.data, pb.ctypes.data)
+    torch.cuda.synchronize()
+    tuned_us = batch.autotune(reps=3)
+    st = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    batch.run(st.cuda_stream)
+    reps = 5
+    e0.record(st)
+    for _ in range(reps):
+        batch.run(st.cuda_stream)
+    e1.record(st)
+    e1.synchronize()
+    batch_us = 1000.0 * e0.elapsed_time(e1) / reps
+    batch.check_errors()
+    pc = np.zeros_like(pa)
+    batch.copy_out(pc.ctypes.data)
+    torch.cuda.synchronize()
+    got = batch.unpack(pc)
+    # the same products through per-product plans (tensor path), sequentially on one stream
+    plans = [polymul.Plan(n, q, 14, tensor=True) for n, q in zip(ns, qs)]
+    da = [torch.from_numpy(x.view(np.int64)).cuda() for x in a]
+    db = [torch.from_numpy(x.view(np.int64)).cuda() for x in b]
+    dc = [torch.empty_like(x) for x in da]
+    for p, x, y, z in zip(plans, da, db, dc):
+        p.multiply(x.data_ptr(), y.data_ptr(), z.data_ptr(), 0, st.cuda_stream)
+    e0.record(st)
+    for _ in range(reps):
+        for p, x, y, z in zip(plans, da, db, dc):
+            p.multiply(x.data_ptr(), y.data_ptr(), z.data_ptr(), 0, st.cuda_stream)
+    e1.record(st)
+    e1.synchronize()
+    seq_us = 1000.0 * e0.elapsed_time(e1) / reps
+    mismatches = sum(int((dc[z].cpu().numpy().view(np.uint64) != got[z]).any(axis=1).sum()) for z in range(K))
+    for p in plans:
+        p.close()
+    batch.close()
+    return {"workload": f"{K} products, N log-uniform over 1024..65536, q widths uniform in 200..868 bits (seed 4)",
+            "us_per_batch": batch_us, "products_per_s": K / (batch_us * 1e-6), "autotuned_us": tuned_us,
+            "per_product_plans_us": seq_us, "per_product_plans_products_per_s": K / (seq_us * 1e-6),
+            "coefficients": int(sum(ns)), "mismatches_vs_per_product_plans": mismatches}
+
+
+SERVE_SIZES = (4096, 16384, 32768, 65536)
+SERVE_WEIGHTS = (0.4, 0.3, 0.2, 0.1)
+
+
+def run_serving(args, torch, polymul):
+    """Poisson arrivals of products of mixed N (868-bit q) through the serving loop,
+    and the same arrival schedule through the plain path one request at a time."""
+    import numpy as np
+
+    rng = np.random.default_rng(5)
+    R = args.serve_requests
+    q = seeded_q(args.seed + 5, args.bits)
+    limbs = (args.bits + 63) // 64
+    sizes = rng.choice(SERVE_SIZES, size=R, p=SERVE_WEIGHTS)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=R))
+    pool_k, ring = 4, 32  # distinct inputs per size; output buffers per size (reused round robin)
+    pools = {}
+    for n in SERVE_SIZES:
+        a = device_inputs(torch, pool_k, n, limbs, q, args.seed + n).cpu().pin_memory()
+        b = device_inputs(torch, pool_k, n, limbs, q, args.seed + 3 * n).cpu().pin_memory()
+        c = torch.zeros((ring, n, limbs), dtype=torch.int64).pin_memory()
+        pools[n] = (a, b, c)
+    last_input = {}  # (n, ring slot) -> input index of the last request written there
+
+    def run(submit, drain):
+        count = {n: 0 for n in SERVE_SIZES}
+        t0 = time.perf_counter()
+        for k in range(R):
+            n = int(sizes[k])
+            j, r = count[n] % pool_k, count[n] % ring
+            count[n] += 1
+            while time.perf_counter() - t0 < arrivals[k]:
+                pass
+            a, b, c = pools[n]
+            submit(n, a[j].data_ptr(), b[j].data_ptr(), c[r].data_ptr(), t0 + arrivals[k])
+            last_input[(n, r)] = j
+        drain()
+        return time.perf_counter() - t0
+
+    # the serving loop
+    srv = polymul.Server(slots=8, max_group=4, tensor=(args.path == "tensor"))
+    for n in SERVE_SIZES:  # plans (tables) resident before the stream starts
+        a, b, c = pools[n]
+        srv.wait(srv.submit_ptr(n, q, limbs, a[0].data_ptr(), b[0].data_ptr(), c[0].data_ptr()))
+    srv.reset_stats()
+    wall = run(lambda n, pa, pb, pc, due: srv.submit_ptr(n, q, limbs, pa, pb, pc), srv.drain)
+    st = srv.stats()
+    srv.close()
+    mismatches = 0
+    plans = {n: polymul.Plan(n, q, limbs) for n in SERVE_SIZES}
+    for (n, r), j in last_input.items():
+        if r >= 2:
+            continue
+        a, b, c = pools[n]
+        want = plans[n].multiply_host(a[j].numpy().view(np.uint64), b[j].numpy().view(np.uint64))
+        mismatches += int((c[r].numpy().view(np.uint64) != want).any(axis=1).sum())
+
+    # the plain path in turn: one pm_multiply_host at a time, same arrival schedule
+    lat = []
+
+    def plain_submit(n, pa, pb, pc, due):
+        polymul.check(polymul.lib().pm_multiply_host(plans[n].handle, pa, pb, pc))
+        lat.append((time.perf_counter() - due) * 1e6)
+
+    plain_wall = run(plain_submit, lambda: None)
+    for p in plans.values():
+        p.close()
+    lat.sort()
+    pct = lambda v, f: v[min(len(v) - 1, int(f * (len(v) - 1) + 0.5))]  # noqa: E731
+    return {
+        "workload": f"{R} requests, Poisson arrivals at {args.serve_rate:.0f}/s (seed 5), N in {SERVE_SIZES} "
+                    f"with weights {SERVE_WEIGHTS}, {args.bits}-bit q, pinned host buffers",
+        "products_per_s": st["products_per_s"], "p50_us": st["p50_us"], "p99_us": st["p99_us"],
+        "mean_us": st["mean_us"], "wall_s": wall, "groups": st["groups"], "peak_inflight": st["peak_inflight"],
+        "peak_group": st["peak_group"], "mismatches": mismatches,
+        "plain_in_turn": {"products_per_s": R / plain_wall, "p50_us": pct(lat, 0.5), "p99_us": pct(lat, 0.99),
+                          "api": "pm_multiply_host, one request at a time"},
+    }
+
+
 def algorithmic_bytes(n, primes, limbs):
     """Mandatory HBM bytes of each kernel per product (SURVEY-style count: inputs
     read once, residue planes written/read once, output written once)."""
@@ -403,6 +551,13 @@ def run_ours(args):
                     "algorithmic_bytes_per_launch": per_launch,
                     "algorithmic_bytes_per_product": alg[dom]}
 
+    serving = None
+    if world == 1 and args.serve_requests > 0:
+        serving = run_serving(args, torch, polymul)
+    uneven = None
+    if world == 1 and args.uneven > 0:
+        uneven = run_uneven(args, torch, polymul)
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         (ca, cb), = host_inputs(n, q, args.seed + 5)
@@ -429,6 +584,8 @@ def run_ours(args):
             "roofline": roofline,
             "kernels": kernels,
             "cpu_baseline": cpu,
+            "serving": serving,
+            "batched_uneven": uneven,
             "clocks": clocks,
             "mismatches": mismatches,
         }

@@ -1,0 +1,174 @@
+// Autotuner: picks a plan's launch shapes by timing them on the plan's own
+// workload (a batch of synthetic products on the plan's device).
+//
+// Knobs (Tuning in pm_internal.h):
+//   row_radix_log    K2 register passes of radix 4 or 8 (more passes with less
+//                    register state, or fewer shared-memory exchanges);
+//   conv_ctas_per_sm persistent CTAs of the tensor conversion per SM;
+//   crt_ctas_per_sm  persistent CTAs of the tensor CRT per SM;
+//   group            products per launch group in batched calls (larger groups
+//                    fill the GPU, smaller ones keep residue planes in L2).
+// Coordinate descent from the defaults, objective = device time per product of
+// a batched call; results are cached per (n, bits(q), coef_limbs, path) for the
+// life of the process, so later plans with the same shape reuse them.
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "../../include/polymul.h"
+#include "pm_internal.h"
+
+namespace pm {
+namespace {
+
+using Key = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, int>;
+std::mutex g_tune_mutex;
+std::map<Key, Tuning> g_tune_cache;
+
+struct Scratch {
+    void* d = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Scratch() {
+        if (st) cudaStreamSynchronize(st);
+        cudaFree(d);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+}  // namespace
+
+Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
+    int device = 0;
+    cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+    const Key key{s.n, s.qbits, s.coef_limbs, s.flags, device};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            s.tune = it->second;
+            if (us_per_product) *us_per_product = -1.0;
+            return s.tune;
+        }
+    }
+    if (reps == 0) reps = 3;
+    // a batch big enough to fill the GPU, capped at ~1.5 GB of buffers
+    const size_t per = 3 * s.io_bytes + s.workspace_bytes;
+    uint32_t count = uint32_t((size_t(1536) << 20) / per);
+    count = count < 1 ? 1 : (count > 16 ? 16 : count);
+    Scratch sc;
+    cuda_check(cudaStreamCreateWithFlags(&sc.st, cudaStreamNonBlocking), "autotune stream");
+    cuda_check(cudaEventCreate(&sc.e0), "autotune event");
+    cuda_check(cudaEventCreate(&sc.e1), "autotune event");
+    cuda_check(cudaMalloc(&sc.d, size_t(count) * per), "autotune buffers");
+    uint8_t* base = static_cast<uint8_t*>(sc.d);
+    // timing does not depend on the values; a fixed byte pattern keeps every kernel on its normal path
+    cuda_check(cudaMemsetAsync(base, 0x5a, size_t(count) * 2 * s.io_bytes, sc.st), "autotune inputs");
+    const uint64_t* a = reinterpret_cast<const uint64_t*>(base);
+    const uint64_t* b = reinterpret_cast<const uint64_t*>(base + size_t(count) * s.io_bytes);
+    uint64_t* c = reinterpret_cast<uint64_t*>(base + size_t(count) * 2 * s.io_bytes);
+    void* ws = base + size_t(count) * 3 * s.io_bytes;
+
+    const Tuning saved = s.tune;
+    auto measure = [&](const Tuning& t) {
+        s.tune = t;
+        uint32_t g = group_size(s);
+        if (g > count) g = count;
+        launch_batch(s, a, b, c, count, g, ws, sc.st);  // warm-up (also function attributes)
+        cuda_check(cudaEventRecord(sc.e0, sc.st), "autotune event");
+        for (uint32_t r = 0; r < reps; ++r) launch_batch(s, a, b, c, count, g, ws, sc.st);
+        cuda_check(cudaEventRecord(sc.e1, sc.st), "autotune event");
+        cuda_check(cudaEventSynchronize(sc.e1), "autotune timing");
+        float ms = 0;
+        cuda_check(cudaEventElapsedTime(&ms, sc.e0, sc.e1), "autotune timing");
+        return 1000.0 * ms / (double(reps) * count);
+    };
+
+    Tuning best;  // defaults
+    best.group = 0;
+    double best_us = measure(best);
+    auto consider = [&](Tuning t) {
+        const double us = measure(t);
+        if (us < best_us) {
+            best_us = us;
+            best = t;
+        }
+    };
+    if (s.logC >= 4) {
+        for (int radix : {2, 3}) {
+            Tuning t = best;
+            t.row_radix_log = radix;
+            if (radix != best.row_radix_log) consider(t);
+        }
+    }
+    if (s.flags & PM_CONVERT_TENSOR) {
+        for (int k : {2, 3, 4}) {
+            Tuning t = best;
+            t.conv_ctas_per_sm = k;
+            if (k != best.conv_ctas_per_sm) consider(t);
+        }
+        for (int k : {1, 2}) {
+            Tuning t = best;
+            t.crt_ctas_per_sm = k;
+            if (k != best.crt_ctas_per_sm) consider(t);
+        }
+    }
+    for (uint32_t g : {1u, 2u, 4u, 8u, 16u}) {
+        if (g > count) break;
+        Tuning t = best;
+        t.group = g;
+        consider(t);
+    }
+    best.tuned = true;
+    s.tune = saved;
+    cuda_check(cudaStreamSynchronize(sc.st), "autotune drain");
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[key] = best;
+    }
+    s.tune = best;
+    if (us_per_product) *us_per_product = best_us;
+    return best;
+}
+
+}  // namespace pm
+
+extern "C" int pm_plan_autotune(pm_plan* plan, uint32_t reps, pm_tuning* chosen) {
+    if (!plan) return pm::fail(PM_ERR_INVALID, "NULL plan");
+    try {
+        double us = 0;
+        const pm::Tuning t = pm::autotune(plan->core, reps, &us);
+        if (chosen) {
+            chosen->row_radix = 1u << t.row_radix_log;
+            chosen->conv_ctas_per_sm = uint32_t(t.conv_ctas_per_sm);
+            chosen->crt_ctas_per_sm = uint32_t(t.crt_ctas_per_sm);
+            chosen->group = t.group;
+            chosen->us_per_product = us;
+        }
+        return PM_OK;
+    } catch (const pm::Failure& f) {
+        return pm::fail(f.status, f.what());
+    } catch (const std::exception& e) {
+        return pm::fail(PM_ERR_INVALID, e.what());
+    }
+}
+
+extern "C" int pm_plan_set_tuning(pm_plan* plan, const pm_tuning* t) {
+    if (!plan || !t) return pm::fail(PM_ERR_INVALID, "NULL argument");
+    if (t->row_radix != 4 && t->row_radix != 8) return pm::fail(PM_ERR_INVALID, "row_radix must be 4 or 8");
+    if (t->conv_ctas_per_sm < 1 || t->conv_ctas_per_sm > 8 || t->crt_ctas_per_sm < 1 || t->crt_ctas_per_sm > 4)
+        return pm::fail(PM_ERR_INVALID, "CTAs per SM out of range");
+    if (t->group > 64) return pm::fail(PM_ERR_INVALID, "group above 64");
+    pm::Tuning& u = plan->core.tune;
+    u.row_radix_log = t->row_radix == 4 ? 2 : 3;
+    u.conv_ctas_per_sm = int(t->conv_ctas_per_sm);
+    u.crt_ctas_per_sm = int(t->crt_ctas_per_sm);
+    u.group = t->group;
+    u.tuned = true;
+    return PM_OK;
+}

@@ -171,39 +171,43 @@ __device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, i
 constexpr int k2_threads(int logc) { return logc >= 12 ? 512 : (logc >= 11 ? 256 : 128); }
 constexpr int k2_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 3 : 7); }
 
-// Rows of C = 2^LOGC >= 8.  grid (R / rows_per_cta, P, count), block
-// rows_per_cta * C/8.  Dynamic shared memory per row: C uint2 forward and C
-// uint2 inverse twiddles, then 2C words of data.  The product overwrites the
-// a plane in place.
-template <int LOGC>
-__global__ void __launch_bounds__(k2_threads(LOGC), k2_min_blocks(LOGC))
-    k2_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
-            const uint2* __restrict__ tw_inv, int n, int logR, int P, size_t ws_bstride) {
+// Rows of C = 2^LOGC >= 8, passes of KP stages (radix 2^KP, KP = 2 or 3; the
+// last forward pass takes the remaining LOGC % KP stages).  grid
+// (R / rows_per_cta, P, count), block rows_per_cta * C/8.  Dynamic shared
+// memory per row: C uint2 forward and C uint2 inverse twiddles, then 2C words
+// of data.  The product overwrites the a plane in place.
+// One row r of prime i of the residue planes at `res` ([2][P][n]); the calling
+// CTA gives each row T = C/8 threads (sub = row slot in the CTA, tid = thread in
+// the row) and 24*C bytes of dynamic shared memory per row slot.
+template <int LOGC, int KP>
+__device__ __forceinline__ void k2_row_body(uint32_t* __restrict__ res, const PrimeConst& pc,
+                                            const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv,
+                                            int n, int logR, int P, int i, int r, int sub, int tid,
+                                            int rows_per_cta) {
     constexpr int C = 1 << LOGC;
     constexpr int T = C / 8;
-    constexpr int NP3 = LOGC / 3;  // radix-8 passes
-    constexpr int REM = LOGC % 3;  // stages of the closing pass
+    constexpr int NP = LOGC / KP;   // full passes
+    constexpr int REM = LOGC % KP;  // stages of the closing pass
+    static_assert(KP == 2 || KP == 3, "pass radix");
     extern __shared__ uint2 smem2[];
-    const int sub = threadIdx.x / T, tid = threadIdx.x % T;
-    const int rows_per_cta = blockDim.x / T;
-    const int r = blockIdx.x * rows_per_cta + sub;
-    const int i = blockIdx.y;
     const int R = 1 << logR;
     uint2* stf = smem2 + sub * 2 * C;
     uint2* sti = stf + C;
     uint32_t* sa = reinterpret_cast<uint32_t*>(smem2 + rows_per_cta * 2 * C) + sub * 2 * C;
     uint32_t* sb = sa + C;
-    const PrimeConst pc = pcs[i];
-    res += blockIdx.z * ws_bstride;
     uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
     const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
+    constexpr int logd0 = LOGC - KP;  // first pass: s0 = 0
 
     uint32_t va[8], vb[8];
 #pragma unroll
-    for (int l = 0; l < 8; ++l) {
-        va[l] = ga[tid + l * T];
-        vb[l] = gb[tid + l * T];
-    }
+    for (int m = 0; m < (8 >> KP); ++m)
+#pragma unroll
+        for (int l = 0; l < (1 << KP); ++l) {
+            const int idx = pass_index<KP>(tid, T, m, l, logd0);
+            va[(m << KP) + l] = ga[idx];
+            vb[(m << KP) + l] = gb[idx];
+        }
     // this row's twiddles: local entry j = 2^s + i' holds Psi_rev[(R + r) 2^s + i']
     {
         const uint2* gf = tw_fwd + size_t(i) * kNMax;
@@ -217,24 +221,23 @@ __global__ void __launch_bounds__(k2_threads(LOGC), k2_min_blocks(LOGC))
         }
     }
     __syncthreads();
-    // forward radix-8 passes
 #pragma unroll
-    for (int q3 = 0; q3 < NP3; ++q3) {
-        const int s0 = 3 * q3, logd = LOGC - s0 - 3;
-        if (q3 > 0) {
-            pass_load<3>(va, sa, tid, T, logd);
-            pass_load<3>(vb, sb, tid, T, logd);
+    for (int q = 0; q < NP; ++q) {
+        const int s0 = KP * q, logd = LOGC - s0 - KP;
+        if (q > 0) {
+            pass_load<KP>(va, sa, tid, T, logd);
+            pass_load<KP>(vb, sb, tid, T, logd);
         }
-        pass_forward<3>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
-        if (q3 + 1 < NP3 || REM) {
+        pass_forward<KP>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
+        if (q + 1 < NP || REM) {
             __syncthreads();
-            pass_store<3>(va, sa, tid, T, logd);
-            pass_store<3>(vb, sb, tid, T, logd);
+            pass_store<KP>(va, sa, tid, T, logd);
+            pass_store<KP>(vb, sb, tid, T, logd);
             __syncthreads();
         }
     }
     if constexpr (REM > 0) {
-        const int s0 = 3 * NP3, logd = 0;
+        const int s0 = KP * NP, logd = 0;
         pass_load<REM>(va, sa, tid, T, logd);
         pass_load<REM>(vb, sb, tid, T, logd);
         pass_forward<REM>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
@@ -247,25 +250,39 @@ __global__ void __launch_bounds__(k2_threads(LOGC), k2_min_blocks(LOGC))
         va[l] = reduce60(uint64_t(x) * y, pc.p, pc.mu);
     }
     if constexpr (REM > 0) {
-        const int s0 = 3 * NP3, logd = 0;
+        const int s0 = KP * NP, logd = 0;
         pass_inverse<REM>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
         __syncthreads();
         pass_store<REM>(va, sa, tid, T, logd);
         __syncthreads();
     }
 #pragma unroll
-    for (int q3 = NP3 - 1; q3 >= 0; --q3) {
-        const int s0 = 3 * q3, logd = LOGC - s0 - 3;
-        if (q3 + 1 < NP3 || REM) pass_load<3>(va, sa, tid, T, logd);
-        pass_inverse<3>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
-        if (q3 > 0) {
+    for (int q = NP - 1; q >= 0; --q) {
+        const int s0 = KP * q, logd = LOGC - s0 - KP;
+        if (q + 1 < NP || REM) pass_load<KP>(va, sa, tid, T, logd);
+        pass_inverse<KP>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
+        if (q > 0) {
             __syncthreads();
-            pass_store<3>(va, sa, tid, T, logd);
+            pass_store<KP>(va, sa, tid, T, logd);
             __syncthreads();
         }
     }
 #pragma unroll
-    for (int l = 0; l < 8; ++l) ga[tid + l * T] = va[l];
+    for (int m = 0; m < (8 >> KP); ++m)
+#pragma unroll
+        for (int l = 0; l < (1 << KP); ++l) ga[pass_index<KP>(tid, T, m, l, logd0)] = va[(m << KP) + l];
+}
+
+template <int LOGC, int KP>
+__global__ void __launch_bounds__(k2_threads(LOGC), k2_min_blocks(LOGC))
+    k2_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
+            const uint2* __restrict__ tw_inv, int n, int logR, int P, size_t ws_bstride) {
+    constexpr int T = (1 << LOGC) / 8;
+    const int sub = threadIdx.x / T, tid = threadIdx.x % T;
+    const int rows_per_cta = blockDim.x / T;
+    const int i = blockIdx.y;
+    k2_row_body<LOGC, KP>(res + blockIdx.z * ws_bstride, pcs[i], tw_fwd, tw_inv, n, logR, P, i,
+                          blockIdx.x * rows_per_cta + sub, sub, tid, rows_per_cta);
 }
 
 // Rows of C <= 4 (N <= 128): one thread per row, everything in registers.

@@ -62,6 +62,15 @@ struct PipelineSlot {
     ~PipelineSlot();
 };
 
+// Launch shapes the autotuner chooses per plan (defaults apply until it runs).
+struct Tuning {
+    int row_radix_log = 3;   // K2 register-pass radix: 2 (radix-4) or 3 (radix-8)
+    int conv_ctas_per_sm = 4;  // K1T persistent CTAs per SM (per prime group share)
+    int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
+    uint32_t group = 0;        // products per launch group in batches (0: fit ~64 MB of residues)
+    bool tuned = false;
+};
+
 // Everything one (n, q) product needs on the device.
 struct PlanCore {
     int device = 0;
@@ -90,10 +99,14 @@ struct PlanCore {
     uint32_t* d_err = nullptr;     // set by a kernel whose bounded wait ran out
     uint32_t tensor_k_crt = 0;
 
+    Tuning tune;
     std::unique_ptr<PipelineSlot> pipe[3];
     uint32_t pipe_group = 0;
 
+    bool tables_only = false;      // set-up for a batch: no own workspace or stream
+
     void init(uint32_t n, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs, uint32_t flags);
+    void init_tables_only(uint32_t n, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs, uint32_t flags);
     void ensure_batch_workspace(uint32_t group);
     void ensure_pipeline(uint32_t group);
     ~PlanCore();

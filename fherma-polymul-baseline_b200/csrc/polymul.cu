@@ -337,9 +337,16 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     cuda_check(cudaMemcpy(d_consts, consts.data(), consts.size() * 4, cudaMemcpyHostToDevice), "upload q");
     cuda_check(cudaMemcpy(d_scale, scale.data(), scale.size() * sizeof(uint2), cudaMemcpyHostToDevice),
                "upload CRT scales");
+    if (flags & PM_CONVERT_TENSOR) tensor_init(*this);
+    if (tables_only) return;
     cuda_check(cudaMalloc(&d_work, workspace_bytes), "allocate residue workspace");
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "create plan stream");
-    if (flags & PM_CONVERT_TENSOR) tensor_init(*this);
+}
+
+void PlanCore::init_tables_only(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t coef_limbs_,
+                                uint32_t flags_) {
+    tables_only = true;
+    init(n_, q64, q_limbs, coef_limbs_, flags_);
 }
 
 void PlanCore::ensure_batch_workspace(uint32_t group) {
@@ -389,7 +396,7 @@ void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, const Batch
                                               int(s.P), int(s.stride), bt.io_bstride, bt.ws_bstride);
 }
 
-template <int LOGC>
+template <int LOGC, int KP>
 void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
     constexpr int C = 1 << LOGC, T = C / 8;
     int rows = T >= 128 ? 1 : 128 / T;
@@ -397,25 +404,33 @@ void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStr
     if (rows > R) rows = R;
     const size_t smem = size_t(rows) * 24 * C;  // 2C uint2 twiddles + 2C words of data per row
     if (smem > 48 * 1024)
-        cuda_check(cudaFuncSetAttribute(k2_rows<LOGC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+        cuda_check(cudaFuncSetAttribute(k2_rows<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "raise K2 shared memory");
     dim3 grid(R / rows, s.P, bt.count), block(rows * T);
-    k2_rows<LOGC><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.n),
+    k2_rows<LOGC, KP><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.n),
                                              int(s.logR), int(s.P), bt.ws_bstride);
+}
+
+template <int LOGC>
+void launch_k2_radix(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
+    if (s.tune.row_radix_log == 2)
+        launch_k2_fixed<LOGC, 2>(s, work, bt, st);
+    else
+        launch_k2_fixed<LOGC, 3>(s, work, bt, st);
 }
 
 void launch_k2(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
     switch (s.logC) {
-        case 12: return launch_k2_fixed<12>(s, work, bt, st);
-        case 3: return launch_k2_fixed<3>(s, work, bt, st);
-        case 4: return launch_k2_fixed<4>(s, work, bt, st);
-        case 5: return launch_k2_fixed<5>(s, work, bt, st);
-        case 6: return launch_k2_fixed<6>(s, work, bt, st);
-        case 7: return launch_k2_fixed<7>(s, work, bt, st);
-        case 8: return launch_k2_fixed<8>(s, work, bt, st);
-        case 9: return launch_k2_fixed<9>(s, work, bt, st);
-        case 10: return launch_k2_fixed<10>(s, work, bt, st);
-        case 11: return launch_k2_fixed<11>(s, work, bt, st);
+        case 12: return launch_k2_radix<12>(s, work, bt, st);
+        case 3: return launch_k2_fixed<3, 3>(s, work, bt, st);
+        case 4: return launch_k2_radix<4>(s, work, bt, st);
+        case 5: return launch_k2_radix<5>(s, work, bt, st);
+        case 6: return launch_k2_radix<6>(s, work, bt, st);
+        case 7: return launch_k2_radix<7>(s, work, bt, st);
+        case 8: return launch_k2_radix<8>(s, work, bt, st);
+        case 9: return launch_k2_radix<9>(s, work, bt, st);
+        case 10: return launch_k2_radix<10>(s, work, bt, st);
+        case 11: return launch_k2_radix<11>(s, work, bt, st);
         default: {
             const int R = 1 << s.logR;
             dim3 grid((R + 31) / 32, s.P, bt.count), block(R < 32 ? R : 32);
@@ -479,6 +494,7 @@ void check_device_errors(const PlanCore& s) {
 // Products whose residue planes fit in about 64 MB run together, so the
 // planes K1 writes are still in L2 when K2 and K3 read them.
 uint32_t group_size(const PlanCore& s) {
+    if (s.tune.group) return s.tune.group;
     const size_t budget = size_t(64) << 20;
     size_t g = budget / s.workspace_bytes;
     if (g < 1) g = 1;

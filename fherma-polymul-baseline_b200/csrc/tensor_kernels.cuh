@@ -1,0 +1,474 @@
+// The tensor-core passes as persistent kernels over an abstract work source.
+//
+// K1T (conversion + forward column stages) and K3T (inverse column stages +
+// CRT) loop over work items; a Work type says how many items there are, what
+// each one is and where its product's data lives:
+//   PlanConvWork / PlanCrtWork   `count` products of one plan, items computed
+//                                from the index (maps are kernel parameters);
+//   TableConvWork / TableCrtWork products of different n and q (an uneven
+//                                batch), items and per-product descriptors read
+//                                from device tables (maps in global memory).
+// Each CTA takes a contiguous chunk of items, so the operand tables it keeps in
+// shared memory (prime-group weights, a product's CRT weights) change rarely.
+//
+// Conversion (reference: rns/tensor_prepare.h:20-101 does the same contraction
+// with WMMA s8 or cuBLAS, centred by -128; unsigned operands need no centring):
+//   D[m][4i+a] = sum_k x_k(m) * byte_a(2^(8k) mod p_i)      k < 128 coefficient bytes
+//   r_i(m)     = sum_a D[m][4i+a] * 2^(8a)  mod p_i          (< 2^48 before the reduction)
+// every D entry is at most 128*255^2 < 2^23, so the s32 accumulation is exact.
+// CRT (the reference accumulates sum t_i (P/p_i mod q) in a 928-bit cuPQC
+// integer, rns/solve.cu:336-420):
+//   A[m][4i+a] = byte_a(t_i(m)),  B[J][4i+a] = byte_J((P/p_i mod q) << 8a)  J < NV
+//                                 B[NV+J][4i+a] = byte_J(floor(2^64/p_i) << 8a)  J < 8
+// every D entry is at most 256*255^2 < 2^24.
+#pragma once
+
+#include <cuda.h>
+
+#include <cstdint>
+
+#include "pm_device.cuh"
+#include "tc_ptx.cuh"
+
+namespace pm {
+
+namespace tc {
+constexpr int kTileM = 128;     // coefficients per tile = 8 columns x 16 rows
+constexpr int kConvGroup = 16;  // primes per conversion MMA (N = 64)
+constexpr int kConvN = 4 * kConvGroup;
+constexpr int kCrtN = 128;      // value bytes + 8 quotient bytes (+ pad)
+constexpr int kCrtK = 256;      // 4 bytes per prime, 64 primes
+constexpr int kMaxPrimes = 64;
+}  // namespace tc
+
+struct ConvItem {
+    int z, pg, poly, cg;
+};
+struct ConvTarget {
+    const CUtensorMap* map;  // coefficient bytes (dims: byte, column, row, product)
+    int mz;                  // product coordinate inside that map
+    uint32_t* res;           // this product's residue planes
+    int n, logC, P;
+};
+struct CrtTarget {
+    const CUtensorMap* map;  // residue planes (dims: column, row, prime, product)
+    int mz;
+    const uint32_t* work;    // the same planes, for rings too small for a tensor map
+    uint32_t* out;           // this product's output coefficients
+    const uint2* scale;
+    const uint32_t* consts;  // q[W], (-P mod q)[W]
+    const uint8_t* crt_w;    // [2][128][128] pre-swizzled CRT weights
+    uint64_t mu_q;
+    int sbits, n, logC, P, stride, use_tma;
+};
+
+// Per-product descriptor of an uneven batch (device table).
+struct BatchProduct {
+    int n, logC, P, W, sbits, stride;
+    uint64_t mu_q;
+    uint64_t io_off;  // u32 words from the batch's a (b, c) base to this product
+    uint64_t ws_off;  // u32 words from the batch's workspace base to its planes
+    const uint2* scale;
+    const uint32_t* consts;
+    const uint8_t* crt_w;
+};
+
+struct PlanConvWork {
+    CUtensorMap map_a, map_b;
+    uint32_t* work;
+    size_t ws_bstride;
+    int n, logC, P, count, pgs;
+    __device__ int groups() const { return (1 << logC) / min(1 << logC, 8); }
+    __device__ int total() const { return pgs * count * 2 * groups(); }
+    __device__ ConvItem item(int k) const {
+        const int per_pg = count * 2 * groups();
+        const int pg = k / per_pg, rest = k - pg * per_pg;
+        return ConvItem{rest / (2 * groups()), pg, (rest / groups()) & 1, rest % groups()};
+    }
+    __device__ ConvTarget target(int z, int poly) const {
+        return ConvTarget{poly ? &map_b : &map_a, z, work + z * ws_bstride, n, logC, P};
+    }
+};
+
+struct TableConvWork {
+    const uint4* items;  // (z, pg, poly, cg)
+    int nitems;
+    const BatchProduct* prod;
+    const CUtensorMap* maps;  // [3 * products]: a, b, residues
+    uint32_t* work;
+    __device__ int total() const { return nitems; }
+    __device__ ConvItem item(int k) const {
+        const uint4 v = items[k];
+        return ConvItem{int(v.x), int(v.y), int(v.z), int(v.w)};
+    }
+    __device__ ConvTarget target(int z, int poly) const {
+        const BatchProduct& d = prod[z];
+        return ConvTarget{maps + 3 * z + poly, 0, work + d.ws_off, d.n, d.logC, d.P};
+    }
+};
+
+struct PlanCrtWork {
+    CUtensorMap map_res;
+    const uint32_t* work;
+    uint32_t* out;
+    size_t ws_bstride, io_bstride;
+    const uint2* scale;
+    const uint32_t* consts;
+    const uint8_t* crt_w;
+    uint64_t mu_q;
+    int sbits, n, logC, P, stride, count, use_tma;
+    __device__ int groups() const { return (1 << logC) / min(1 << logC, 8); }
+    __device__ int total() const { return count * groups(); }
+    __device__ int2 item(int k) const { return make_int2(k / groups(), k % groups()); }
+    __device__ CrtTarget target(int z) const {
+        return CrtTarget{&map_res, z, work + z * ws_bstride, out + z * io_bstride, scale, consts, crt_w, mu_q,
+                         sbits, n, logC, P, stride, use_tma};
+    }
+};
+
+struct TableCrtWork {
+    const uint2* items;  // (z, cg)
+    int nitems;
+    const BatchProduct* prod;
+    const CUtensorMap* maps;
+    const uint32_t* work;
+    uint32_t* out;
+    __device__ int total() const { return nitems; }
+    __device__ int2 item(int k) const {
+        const uint2 v = items[k];
+        return make_int2(int(v.x), int(v.y));
+    }
+    __device__ CrtTarget target(int z) const {
+        const BatchProduct& d = prod[z];
+        return CrtTarget{maps + 3 * z + 2, 0, work + d.ws_off, out + d.io_off, d.scale, d.consts, d.crt_w,
+                         d.mu_q, d.sbits, d.n, d.logC, d.P, d.stride, 1};
+    }
+};
+
+// ---------------------------------------------------------------------------
+// K1T: tensor-core conversion + forward column stages, persistent.  Block 128.
+// A tile holds coefficient r*C + Gc*cg + c of one polynomial in row m = r*Gc + c
+// and arrives by TMA (box: 128 bytes x Gc columns x R rows, 128-byte swizzle,
+// bytes past the coefficient width zero-filled), double-buffered so the next
+// item loads while this one is converted.  Items are ordered prime group
+// first; the group's pre-swizzled weights (B), constants and column twiddles
+// are reloaded when the group changes.
+// Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose 16x128 words.
+// ---------------------------------------------------------------------------
+template <int LOGR, class Work>
+__global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work w,
+                                                   const PrimeConst* __restrict__ pcs,
+                                                   const uint8_t* __restrict__ conv_w,
+                                                   const uint2* __restrict__ tw_fwd, uint32_t* __restrict__ err) {
+    constexpr int R = 1 << LOGR;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = sbase;                        // 2 x (128 x 128 B)
+    uint8_t* sB = sbase + 32768;                // 64 x 128 B
+    uint32_t* sT = reinterpret_cast<uint32_t*>(sbase + 32768 + 8192);  // [16][128] residues
+    __shared__ uint64_t tma_bar[2], mma_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ PrimeConst spc[tc::kConvGroup];
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int total = w.total();
+    const int chunk = (total + int(gridDim.x) - 1) / int(gridDim.x);
+    const int begin = int(blockIdx.x) * chunk;
+    const int end = min(total, begin + chunk);
+
+    for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 64);
+    if (tid == 0) {
+        tc::mbar_init(&tma_bar[0], 1);
+        tc::mbar_init(&tma_bar[1], 1);
+        tc::mbar_init(&mma_bar, 1);
+    }
+    tc::fence_smem_async();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tbase = tmem_base;
+    const uint32_t taddr = tbase + (uint32_t(32 * (warp & 3)) << 16);
+
+    auto issue = [&](int k, int buf) {
+        const ConvItem it = w.item(k);
+        const ConvTarget t = w.target(it.z, it.poly);
+        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+        tc::mbar_expect_tx(&tma_bar[buf], 128u * uint32_t(Gc) * uint32_t(R));
+        tc::tma_load_4d(sA + buf * 16384, t.map, 0, it.cg * Gc, 0, t.mz, &tma_bar[buf]);
+    };
+    if (tid == 0 && begin < end) issue(begin, 0);
+
+    // column-stage role: prime j of the group, column c of the tile
+    const int cj = tid / 8, cc = tid % 8;
+    uint2 twr[R > 1 ? R - 1 : 1];
+    PrimeConst cpc{};
+    int cur_pg = -1;
+
+    uint32_t tma_phases = 0, mma_phase = 0;  // bit b: parity of buffer b's next TMA completion
+    bool ok = true;
+    int kk = 0;
+    for (int k = begin; k < end; ++k, ++kk) {
+        const ConvItem it = w.item(k);
+        const ConvTarget t = w.target(it.z, it.poly);
+        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+        if (it.pg != cur_pg) {  // all earlier MMAs are complete: B may be rewritten
+            const uint4* src = reinterpret_cast<const uint4*>(conv_w + size_t(it.pg) * 8192);
+            for (int q = tid; q < 512; q += 128) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
+            if (tid < tc::kConvGroup) spc[tid] = pcs[it.pg * tc::kConvGroup + tid];
+            const int ci = it.pg * tc::kConvGroup + cj;
+#pragma unroll
+            for (int q = 1; q < R; ++q) twr[q - 1] = __ldg(tw_fwd + size_t(ci) * kNMax + q);
+            cpc = pcs[ci];
+            cur_pg = it.pg;
+            tc::fence_smem_async();
+            __syncthreads();
+        }
+        const int np = min(tc::kConvGroup, t.P - it.pg * tc::kConvGroup);
+        const int buf = kk & 1;
+        if (tid == 0) {
+            ok = tc::mbar_wait(&tma_bar[buf], (tma_phases >> buf) & 1u) && ok;
+            tc::fence_after();
+            const uint32_t a0 = tc::smem_u32(sA + buf * 16384), b0 = tc::smem_u32(sB);
+            constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kConvN);
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks)
+                tc::mma_u8(tbase, tc::sw128_desc(a0 + 32 * ks), tc::sw128_desc(b0 + 32 * ks), idesc, ks > 0);
+            tc::mma_commit(&mma_bar);
+            // the other buffer's last reader was the previous item's MMA, already complete
+            if (k + 1 < end) issue(k + 1, buf ^ 1);
+        }
+        tma_phases ^= 1u << buf;
+        ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
+        mma_phase ^= 1;
+        tc::fence_after();
+        // --- residues of row m = tid for the group's 16 primes ---
+#pragma unroll
+        for (int q4 = 0; q4 < 4; ++q4) {
+            uint32_t d[16];
+            tc::tmem_ld16(taddr + 16 * q4, d);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = 4 * q4 + u;
+                const uint64_t v = uint64_t(d[4 * u]) + (uint64_t(d[4 * u + 1]) << 8) +
+                                   (uint64_t(d[4 * u + 2]) << 16) + (uint64_t(d[4 * u + 3]) << 24);
+                sT[j * 128 + tid] = reduce60(v, spc[j].p, spc[j].mu);
+            }
+        }
+        tc::fence_before();
+        __syncthreads();
+        // --- forward column stages in registers, then store ---
+        if (cj < np && cc < Gc) {
+            const int ci = it.pg * tc::kConvGroup + cj;
+            uint32_t v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = sT[cj * 128 + r * Gc + cc];
+#pragma unroll
+            for (int s = 0; s < LOGR; ++s) {
+                const int h = R >> (s + 1);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (!(r & h)) ct_bfly(v[r], v[r + h], twr[(1 << s) + (r >> (LOGR - s)) - 1], cpc.p, cpc.two_p);
+            }
+            uint32_t* dst = t.res + (size_t(it.poly) * t.P + ci) * t.n + size_t(it.cg) * Gc + cc;
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst[size_t(r) << t.logC] = v[r];
+        }
+        __syncthreads();  // sT is rewritten by the next item
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after();
+        tc::tmem_dealloc(tbase, 64);
+    }
+    if (!ok && tid == 0) atomicOr(err, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// K3T: inverse column stages + CRT on the tensor cores, persistent.  Block 128.
+// An item's residues for every prime arrive by TMA (box: Gc columns x R rows x
+// P primes of u32); the next item's box is requested as soon as this one has
+// been turned into CRT digits, so it loads during the MMA and the epilogue.
+// The CRT weights, q constants and column twiddles of the current product stay
+// in shared memory until an item of another product needs its own.
+// Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB,
+// residue box 64*R*8 words, inverse column twiddles 64*(R-1) uint2.
+// ---------------------------------------------------------------------------
+template <int LOGR, int W, class Work>
+__global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs,
+                                               const uint2* __restrict__ tw_inv, uint32_t* __restrict__ err) {
+    constexpr int R = 1 << LOGR;
+    constexpr int RT = R > 1 ? R - 1 : 1;
+    constexpr int NV = 4 * W + 4;  // value byte columns
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = sbase;                                        // [2][128][128 B]
+    uint8_t* sB = sbase + 32768;                                // [2][128][128 B]
+    uint32_t* sR = reinterpret_cast<uint32_t*>(sbase + 65536);  // [P][R][Gc]
+    uint2* sTw = reinterpret_cast<uint2*>(sR + tc::kMaxPrimes * R * 8);  // [P][R-1]
+    __shared__ uint64_t tma_bar, mma_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ uint32_t s_q[2 * W];
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int total = w.total();
+    const int chunk = (total + int(gridDim.x) - 1) / int(gridDim.x);
+    const int begin = int(blockIdx.x) * chunk;
+    const int end = min(total, begin + chunk);
+
+    for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
+    if (tid == 0) {
+        tc::mbar_init(&tma_bar, 1);
+        tc::mbar_init(&mma_bar, 1);
+    }
+    tc::fence_smem_async();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tbase = tmem_base;
+    const uint32_t taddr = tbase + (uint32_t(32 * (warp & 3)) << 16);
+
+    auto issue = [&](int k) {
+        const int2 it = w.item(k);
+        const CrtTarget t = w.target(it.x);
+        if (!t.use_tma) return;
+        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+        tc::mbar_expect_tx(&tma_bar, uint32_t(t.P * R * Gc) * 4u);
+        tc::tma_load_4d(sR, t.map, it.y * Gc, 0, 0, t.mz, &tma_bar);
+    };
+    if (tid == 0 && begin < end) issue(begin);
+
+    const uint8_t* cur_w = nullptr;  // the product whose tables are in shared memory
+    int cur_P = 0;
+    uint32_t tma_phase = 0, mma_phase = 0;
+    bool ok = true;
+    for (int k = begin; k < end; ++k) {
+        const int2 it = w.item(k);
+        const CrtTarget t = w.target(it.x);
+        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+        const int cg = it.y;
+        if (t.crt_w != cur_w || t.P != cur_P) {  // the previous item's MMA is complete: B may be rewritten
+            const uint4* src = reinterpret_cast<const uint4*>(t.crt_w);
+            for (int q = tid; q < 2048; q += 128) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
+            for (int q = tid; q < 2 * W; q += 128) s_q[q] = t.consts[q];
+            if (R > 1)
+                for (int q = tid; q < t.P * RT; q += 128)
+                    sTw[q] = __ldg(tw_inv + size_t(q / RT) * kNMax + 1 + q % RT);
+            if (t.P != cur_P)  // K columns of absent primes must read as zero
+                for (int q = tid; q < 2048; q += 128) reinterpret_cast<uint4*>(sA)[q] = make_uint4(0, 0, 0, 0);
+            cur_w = t.crt_w;
+            cur_P = t.P;
+            tc::fence_smem_async();
+            __syncthreads();
+        }
+        if (t.use_tma) {
+            ok = tc::mbar_wait(&tma_bar, tma_phase) && ok;
+            tma_phase ^= 1;
+        } else {
+            const int box = t.P * R * Gc;
+            for (int q = tid; q < box; q += 128) {
+                const int c = q % Gc, r = (q / Gc) % R, i = q / (Gc * R);
+                sR[q] = t.work[size_t(i) * t.n + (size_t(r) << t.logC) + size_t(cg) * Gc + c];
+            }
+            __syncthreads();
+        }
+        // --- inverse column stages and CRT digits into A ---
+        const int pairs = t.P * Gc;
+        for (int pr = tid; pr < pairs; pr += 128) {
+            const int i = pr / Gc, c = pr - i * Gc;
+            const PrimeConst pc = pcs[i];
+            uint32_t v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = sR[(i * R + r) * Gc + c];
+            const uint2* tw = sTw + i * RT - 1;  // tw[k] = Psi_inv_rev[k], k >= 1
+#pragma unroll
+            for (int s = LOGR - 1; s >= 0; --s) {
+                const int h = R >> (s + 1);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (!(r & h)) gs_bfly(v[r], v[r + h], tw[(1 << s) + (r >> (LOGR - s))], pc.p, pc.two_p);
+            }
+            const uint2 sc = __ldg(t.scale + i);
+            const uint32_t ka = uint32_t(i) >> 5, kb = (4u * i) & 127u;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t x = csub(shoup_mul(v[r], sc, pc.p), pc.p);
+                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(c * R + r, kb)) = x;
+            }
+        }
+        tc::fence_smem_async();
+        tc::fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after();
+            // the residue box is free again: fetch the next item's during the MMA and epilogue
+            if (k + 1 < end) issue(k + 1);
+            const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+            constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kCrtN);
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const uint32_t off = (ks >> 2) * 16384 + 32 * (ks & 3);
+                tc::mma_u8(tbase, tc::sw128_desc(a0 + off), tc::sw128_desc(b0 + off), idesc, ks > 0);
+            }
+            tc::mma_commit(&mma_bar);
+        }
+        ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
+        mma_phase ^= 1;
+        tc::fence_after();
+        // --- carry-propagate the byte columns of row m = tid ---
+        // value: NV/4 = W+1 words plus the carry-out; quotient estimate: 8 columns
+        uint32_t acc[W + 2];
+        uint64_t carry = 0;
+        uint64_t fsum0 = 0, fsum1 = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            uint32_t d[16];
+            tc::tmem_ld16(taddr + 16 * q, d);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int J = 16 * q + 4 * u;  // first byte column of this 32-bit word
+                const uint64_t s = uint64_t(d[4 * u]) + (uint64_t(d[4 * u + 1]) << 8) +
+                                   (uint64_t(d[4 * u + 2]) << 16) + (uint64_t(d[4 * u + 3]) << 24);
+                if (J < NV) {
+                    const uint64_t x = s + carry;
+                    acc[J / 4] = uint32_t(x);
+                    carry = x >> 32;
+                } else if (J == NV) {
+                    fsum0 = s;
+                } else if (J == NV + 4) {
+                    fsum1 = s;
+                }
+            }
+        }
+        acc[W + 1] = uint32_t(carry);
+        const uint64_t f1 = fsum1 + (fsum0 >> 32);
+        // nearest integer of sum t_i / p_i: (f1 * 2^32 + low) / 2^64 rounded
+        const uint32_t nearest = uint32_t(f1 >> 32) + (uint32_t(f1) >> 31);
+        const int cc = tid / R, rr = tid % R;
+        if (cc < Gc) {
+            const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
+            crt_finish<W>(acc, nearest, s_q, t.mu_q, t.sbits, t.out + J * t.stride, t.stride);
+        }
+        tc::fence_before();
+        __syncthreads();
+    }
+    if (warp == 0) {
+        tc::fence_after();
+        tc::tmem_dealloc(tbase, 128);
+    }
+    if (!ok && tid == 0) atomicOr(err, 1u);
+}
+
+// shared-memory bytes the kernels above ask for
+constexpr size_t k1t_smem_bytes() { return 1024 + 32768 + 8192 + 16 * 128 * 4; }
+template <int LOGR>
+constexpr size_t k3t_smem_bytes() {
+    return 1024 + 65536 + size_t(tc::kMaxPrimes) * (1 << LOGR) * 8 * 4 +
+           size_t(tc::kMaxPrimes) * ((1 << LOGR) > 1 ? (1 << LOGR) - 1 : 1) * 8;
+}
+
+}  // namespace pm

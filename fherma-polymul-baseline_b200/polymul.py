@@ -43,6 +43,11 @@ class PlanInfo(ctypes.Structure):
                 ("workspace_bytes", ctypes.c_size_t)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("row_radix", ctypes.c_uint32), ("conv_ctas_per_sm", ctypes.c_uint32),
+                ("crt_ctas_per_sm", ctypes.c_uint32), ("group", ctypes.c_uint32), ("us_per_product", ctypes.c_double)]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_uint32), ("max_group", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32), ("device_budget_bytes", ctypes.c_size_t)]
@@ -80,6 +85,17 @@ def lib():
         L.pm_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
         L.pm_server_reset_stats.argtypes = [vp]
         L.pm_server_destroy.argtypes = [vp]
+        L.pm_plan_autotune.argtypes = [vp, u32, ctypes.POINTER(Tuning)]
+        L.pm_plan_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.pm_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(u32), ctypes.POINTER(u64p),
+                                      ctypes.POINTER(u32), u32]
+        L.pm_batch_buffers.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), u64p]
+        L.pm_batch_copy_in.argtypes = [vp, vp, vp, vp]
+        L.pm_batch_copy_out.argtypes = [vp, vp, vp]
+        L.pm_batch_run.argtypes = [vp, vp]
+        L.pm_batch_check.argtypes = [vp]
+        L.pm_batch_autotune.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_double)]
+        L.pm_batch_destroy.argtypes = [vp]
         L.pm_status_string.restype = ctypes.c_char_p
         L.pm_status_string.argtypes = [ctypes.c_int]
         L.pm_last_error.restype = ctypes.c_char_p
@@ -182,6 +198,16 @@ class Plan:
         check(lib().pm_multiply_host(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
         return c
 
+    def autotune(self, reps=3):
+        """Time candidate launch shapes and keep the fastest; returns them as a dict."""
+        t = Tuning()
+        check(lib().pm_plan_autotune(self._h, reps, ctypes.byref(t)))
+        return {name: getattr(t, name) for name, _ in Tuning._fields_}
+
+    def set_tuning(self, row_radix=8, conv_ctas_per_sm=4, crt_ctas_per_sm=2, group=0):
+        t = Tuning(row_radix, conv_ctas_per_sm, crt_ctas_per_sm, group, 0.0)
+        check(lib().pm_plan_set_tuning(self._h, ctypes.byref(t)))
+
     def multiply_host_batch(self, a, b, out=None):
         """(count, n, limbs) host arrays -> products, pipelined over three streams; synchronous."""
         a = np.ascontiguousarray(a, dtype=np.uint64)
@@ -248,6 +274,82 @@ class Server:
     def close(self):
         if self._h:
             lib().pm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Batch:
+    """Uneven batch (pm_batch_*): products of different n and q run as one CUDA graph."""
+
+    def __init__(self, ns, qs, coef_limbs=14):
+        count = len(ns)
+        self.ns = [int(n) for n in ns]
+        self.coef_limbs = int(coef_limbs)
+        self._qarr = [q_limbs_of(q) for q in qs]
+        n_arr = (ctypes.c_uint32 * count)(*self.ns)
+        q_ptrs = (ctypes.POINTER(ctypes.c_uint64) * count)(
+            *[qa.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)) for qa in self._qarr])
+        ql = (ctypes.c_uint32 * count)(*[len(qa) for qa in self._qarr])
+        self._h = ctypes.c_void_p()
+        check(lib().pm_batch_create(ctypes.byref(self._h), count, n_arr, q_ptrs, ql, self.coef_limbs))
+        offs = (ctypes.c_uint64 * count)()
+        a, b, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib().pm_batch_buffers(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), offs))
+        self.offsets = [int(o) for o in offs]
+        self.words = sum(n * self.coef_limbs for n in self.ns)
+        self.a_ptr, self.b_ptr, self.c_ptr = a.value, b.value, c.value
+
+    def pack(self, arrays):
+        """List of (n_z, limbs) arrays -> one packed uint64 array in the batch's layout."""
+        out = np.zeros(self.words, dtype=np.uint64)
+        for off, arr in zip(self.offsets, arrays):
+            flat = np.ascontiguousarray(arr, dtype=np.uint64).ravel()
+            out[off:off + flat.size] = flat
+        return out
+
+    def unpack(self, packed):
+        return [packed[off:off + n * self.coef_limbs].reshape(n, self.coef_limbs)
+                for off, n in zip(self.offsets, self.ns)]
+
+    def copy_in(self, a_packed_ptr, b_packed_ptr, stream=0):
+        check(lib().pm_batch_copy_in(self._h, a_packed_ptr, b_packed_ptr, stream or None))
+
+    def copy_out(self, c_packed_ptr, stream=0):
+        check(lib().pm_batch_copy_out(self._h, c_packed_ptr, stream or None))
+
+    def run(self, stream=0):
+        check(lib().pm_batch_run(self._h, stream or None))
+
+    def check_errors(self):
+        check(lib().pm_batch_check(self._h))
+
+    def autotune(self, reps=3):
+        us = ctypes.c_double(0)
+        check(lib().pm_batch_autotune(self._h, reps, ctypes.byref(us)))
+        return us.value
+
+    def multiply_host(self, a_list, b_list):
+        """Synchronous convenience: host arrays in, list of products out."""
+        import torch
+
+        a = self.pack(a_list)
+        b = self.pack(b_list)
+        c = np.zeros_like(a)
+        self.copy_in(a.ctypes.data, b.ctypes.data)
+        self.run()
+        self.copy_out(c.ctypes.data)
+        torch.cuda.synchronize()
+        self.check_errors()
+        return self.unpack(c)
+
+    def close(self):
+        if self._h:
+            lib().pm_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

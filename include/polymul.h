@@ -67,6 +67,25 @@ int pm_plan_create(pm_plan** plan, uint32_t n, const uint64_t* q, uint32_t q_lim
 
 int pm_plan_get_info(const pm_plan* plan, pm_plan_info* info);
 
+/* Launch shapes of a plan (see pm_plan_autotune). */
+typedef struct {
+    uint32_t row_radix;         /* radix of the row NTT register passes: 4 or 8 */
+    uint32_t conv_ctas_per_sm;  /* persistent CTAs of the tensor conversion per SM, 1..8 */
+    uint32_t crt_ctas_per_sm;   /* persistent CTAs of the tensor CRT per SM, 1..4 */
+    uint32_t group;             /* products per launch group in batched calls (0: fit ~64 MB of residues) */
+    double us_per_product;      /* device time the autotuner measured (-1: taken from its cache) */
+} pm_tuning;
+
+/*
+ * Time candidate launch shapes on a synthetic batch of this plan's products
+ * (allocates temporary device memory; set-up time, not a hot-path call) and
+ * keep the fastest.  Results are cached per (n, bits(q), coef_limbs, flags)
+ * for the process.  Results of the products never depend on the tuning.
+ */
+int pm_plan_autotune(pm_plan* plan, uint32_t reps, pm_tuning* chosen);
+/* Apply launch shapes directly (us_per_product is ignored). */
+int pm_plan_set_tuning(pm_plan* plan, const pm_tuning* tuning);
+
 /* Replaces fherma_free (fherma.h:46; rns/solve.cu:854). */
 int pm_plan_destroy(pm_plan* plan);
 
@@ -132,6 +151,36 @@ int pm_multiply_host_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, 
  * sets *count.  Mirrors rns::setup's prime search (rns/host_setup.h:67-83).
  */
 int pm_basis_query(uint32_t n, uint32_t q_bits, uint32_t* primes, uint32_t capacity, uint32_t* count);
+
+/* ------------------------------------------------------------------------
+ * Uneven batches: `count` products of different n (256..65536) and different
+ * odd q, all on the tensor path, run as one CUDA graph of persistent kernels
+ * over flat work tables (conversion items ordered by prime group, row items per
+ * ring size, CRT items per width).  The batch owns packed device buffers:
+ * product z's a, b, c start offsets[z] u64 words into the buffers returned by
+ * pm_batch_buffers, each n_z x coef_limbs.  No counterpart in the reference.
+ * ------------------------------------------------------------------------ */
+typedef struct pm_batch pm_batch;
+/* q[z] points to q_limbs[z] u64 words; coef_limbs is shared and even. */
+int pm_batch_create(pm_batch** batch, uint32_t count, const uint32_t* n, const uint64_t* const* q,
+                    const uint32_t* q_limbs, uint32_t coef_limbs);
+int pm_batch_buffers(pm_batch* batch, uint64_t** a, uint64_t** b, uint64_t** c, uint64_t* offsets);
+/* Copy all products' a and b in (host or device arrays in the batch's packing:
+   product z at offsets[z] u64 words), or all c out; asynchronous on `stream`. */
+int pm_batch_copy_in(pm_batch* batch, const uint64_t* a, const uint64_t* b, pm_stream stream);
+int pm_batch_copy_out(pm_batch* batch, uint64_t* c, pm_stream stream);
+/* One graph launch, asynchronous on `stream`. */
+int pm_batch_run(pm_batch* batch, pm_stream stream);
+/* After the stream is idle: PM_ERR_TIMEOUT if a kernel's bounded wait ran out. */
+int pm_batch_check(pm_batch* batch);
+/*
+ * Re-time the batch graph under candidate launch shapes (row-pass radix per
+ * ring size, persistent grid sizes of the conversion and CRT phases), keep the
+ * fastest and re-capture; *us_per_run gets its device time.  Set-up time, not a
+ * hot-path call; results never depend on it.
+ */
+int pm_batch_autotune(pm_batch* batch, uint32_t reps, double* us_per_run);
+int pm_batch_destroy(pm_batch* batch);
 
 /* ------------------------------------------------------------------------
  * Serving: products submitted one by one from host threads, admitted onto the

@@ -201,3 +201,33 @@ def test_host_batch_pipeline(cuda, path, pinned):
             assert (got[k] == p.multiply_host(a[k], b[k])).all(), k
     for k in (0, count - 1):
         assert (got[k] == oracle.rns_multiply(a[k], b[k], q)).all()
+
+
+@pytest.mark.parametrize("n", [4096, 32768])
+def test_tunings_do_not_change_results(cuda, path, n):
+    """Every launch shape the autotuner may pick gives the same bits."""
+    torch = cuda
+    rng = np.random.default_rng(n + 17)
+    q = random_q(rng, 868)
+    count = 5
+    a = torch.from_numpy(np.stack([uniform_below(rng, q, n, 14) for _ in range(count)]).view(np.int64)).cuda()
+    b = torch.from_numpy(np.stack([uniform_below(rng, q, n, 14) for _ in range(count)]).view(np.int64)).cuda()
+    ref = None
+    with make_plan(path, n, q, 14) as p:
+        for radix, conv, crt, group in [(8, 4, 2, 0), (4, 4, 2, 0), (8, 2, 1, 1), (4, 3, 1, 2), (8, 4, 2, 5)]:
+            p.set_tuning(radix, conv, crt, group)
+            c = torch.zeros_like(a)
+            p.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), count)
+            torch.cuda.synchronize()
+            if ref is None:
+                ref = c.clone()
+            assert torch.equal(c, ref), (radix, conv, crt, group)
+        chosen = p.autotune()
+        assert chosen["row_radix"] in (4, 8) and chosen["us_per_product"] > 0
+        c = torch.zeros_like(a)
+        p.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), count)
+        torch.cuda.synchronize()
+        assert torch.equal(c, ref)
+    for k in (0, count - 1):
+        ak, bk = a[k].cpu().numpy().view(np.uint64), b[k].cpu().numpy().view(np.uint64)
+        assert (ref[k].cpu().numpy().view(np.uint64) == oracle.rns_multiply(ak, bk, q)).all()
