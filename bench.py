@@ -56,6 +56,8 @@ def parse():
                     help="requests in the serving stream (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=6000.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--uneven", type=int, default=64, help="products in the uneven batch (0 skips it)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default launch shapes instead of the autotuner's")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="K",
                     help="no timing: run K single products (one launch sequence each) for an ncu capture")
     return ap.parse_args()
@@ -441,6 +443,7 @@ def run_ours(args):
     q = seeded_q(args.seed, bits)
     limbs = (bits + 63) // 64
     plan = polymul.Plan(n, q, coef_limbs=limbs, tensor=(args.path == "tensor"))
+    tuning = plan.autotune(reps=3) if args.autotune else None
     B = args.batch
     A = device_inputs(torch, B, n, limbs, q, args.seed + 17 + 1000 * rank)
     Bv = device_inputs(torch, B, n, limbs, q, args.seed + 29 + 1000 * rank)
@@ -558,6 +561,25 @@ def run_ours(args):
     if world == 1 and args.uneven > 0:
         uneven = run_uneven(args, torch, polymul)
 
+    # K2 is bound by instruction issue, not by HBM: butterflies per second against the issue
+    # bound of one warp instruction per SM sub-partition per clock (128 thread instructions
+    # per SM per clock) at 7 instructions per lazy Harvey butterfly (2 IADD, 1 IMNMX,
+    # 3 IMAD incl. the high product, 1 IADD3), at the clock sampled during the timed region
+    alu = None
+    if "k2_rows" in prof:
+        cnt, tot = prof["k2_rows"]
+        logr = 4 if args.path == "tensor" else 5
+        rows_stages = (n.bit_length() - 1) - logr
+        bfly = 3 * plan.primes * (n // 2) * rows_stages  # a, b forward + inverse, row stages only
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clocks.get("sm_mhz") or 1965.0
+        peak_bfly = 128.0 / 7.0 * sms * mhz * 1e6
+        achieved = bfly * timed_products / (tot / 1000.0)
+        alu = {"kernel": "k2_rows", "butterflies_per_product": bfly, "achieved_per_s": achieved,
+               "peak_per_s": peak_bfly, "frac": achieved / peak_bfly,
+               "unit": "butterflies/s", "sm_mhz": mhz,
+               "model": "issue bound: 7 thread instructions per lazy butterfly, 128 per SM per clock"}
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         (ca, cb), = host_inputs(n, q, args.seed + 5)
@@ -577,11 +599,13 @@ def run_ours(args):
                        "n": n, "q_bits": bits, "batch": B, "primes": plan.primes,
                        "path": args.path,
                        "l2": f"inputs larger than L2: {2 * B * io / 1e9:.2f} GB of a, b read per step",
-                       "parallelism": f"replicas x{world}", "oracle_check": f"{checked} products bit-exact"},
+                       "parallelism": f"replicas x{world}", "oracle_check": f"{checked} products bit-exact",
+                       "tuning": tuning},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * E * io, "d2h_bytes_per_step": E * io,
                     "api": "pm_multiply_host_batch, pinned host buffers", "products_per_step": E},
             "gpu_launches": launches,
             "roofline": roofline,
+            "alu_roofline": alu,
             "kernels": kernels,
             "cpu_baseline": cpu,
             "serving": serving,

@@ -1,10 +1,14 @@
-"""Writes crt_mac.cuh: acc[0..W+1] += t * m[0..W-1] as one PTX carry chain per
-width W (two chains: the low halves of t*m[k] into acc[k], the high halves into
-acc[k+1]).  Run: python gen_crt_mac.py > crt_mac.cuh"""
+"""Writes crt_mac.cuh: multiword helpers as single PTX carry chains, one
+specialization per width W (python gen_crt_mac.py > crt_mac.cuh):
+
+  crt_mac<W>(a[W+2], t, m[W])       a += t * m           (low halves into a[k], high halves into a[k+1])
+  mp_sub<N>(a[N], b[N]) -> mask     a -= b, mask = 0xffffffff if it borrowed out, else 0
+  mp_sub_hi<W>(a[W+2], b[W+2])      a -= b * 2^32 (b[W+1] must be 0)
+"""
 WIDTHS = [4, 8, 12, 16, 20, 24, 28]
 
 
-def body(W):
+def mac_body(W):
     acc = [f"%{i}" for i in range(W + 2)]
     m = [f"%{W + 2 + i}" for i in range(W)]
     t = f"%{2 * W + 2}"
@@ -17,17 +21,52 @@ def body(W):
     return "\\n\\t".join(lo + hi)
 
 
+def sub_body(N):
+    a = [f"%{i + 1}" for i in range(N)]
+    b = [f"%{N + 1 + i}" for i in range(N)]
+    lines = [f"sub.cc.u32 {a[0]}, {a[0]}, {b[0]};"]
+    lines += [f"subc.cc.u32 {a[k]}, {a[k]}, {b[k]};" for k in range(1, N)]
+    lines += ["subc.u32 %0, 0, 0;"]
+    return "\\n\\t".join(lines)
+
+
+def sub_hi_body(W):
+    n = W + 2
+    a = [f"%{i}" for i in range(n)]
+    b = [f"%{n + i}" for i in range(n - 1)]
+    lines = [f"sub.cc.u32 {a[1]}, {a[1]}, {b[0]};"]
+    lines += [f"subc.cc.u32 {a[k]}, {a[k]}, {b[k - 1]};" for k in range(2, n)]
+    return "\\n\\t".join(lines)
+
+
 def main():
     out = ["// Generated by gen_crt_mac.py -- do not edit.",
-           "// acc (W+2 words) += t * m (W words), exact, as PTX carry chains.",
+           "// Multiword arithmetic as PTX carry chains (see the generator for the contracts).",
            "#pragma once", "#include <cstdint>", "namespace pm {",
-           "template <int W> __device__ __forceinline__ void crt_mac(uint32_t (&a)[W + 2], uint32_t t, const uint32_t (&m)[W]);"]
+           "template <int W> __device__ __forceinline__ void crt_mac(uint32_t (&a)[W + 2], uint32_t t, const uint32_t (&m)[W]);",
+           "template <int N> __device__ __forceinline__ uint32_t mp_sub(uint32_t (&a)[N], const uint32_t (&b)[N]);",
+           "template <int W> __device__ __forceinline__ void mp_sub_hi(uint32_t (&a)[W + 2], const uint32_t (&b)[W + 2]);"]
     for W in WIDTHS:
         outs = ", ".join(f'"+r"(a[{i}])' for i in range(W + 2))
         ins = ", ".join(f'"r"(m[{i}])' for i in range(W)) + ', "r"(t)'
         out.append(f"template <> __device__ __forceinline__ void crt_mac<{W}>(uint32_t (&a)[{W + 2}], uint32_t t, "
                    f"const uint32_t (&m)[{W}]) {{")
-        out.append(f'    asm("{body(W)}"\n        : {outs}\n        : {ins});')
+        out.append(f'    asm("{mac_body(W)}"\n        : {outs}\n        : {ins});')
+        out.append("}")
+        N = W + 2
+        outs = '"=r"(mask), ' + ", ".join(f'"+r"(a[{i}])' for i in range(N))
+        ins = ", ".join(f'"r"(b[{i}])' for i in range(N))
+        out.append(f"template <> __device__ __forceinline__ uint32_t mp_sub<{N}>(uint32_t (&a)[{N}], "
+                   f"const uint32_t (&b)[{N}]) {{")
+        out.append("    uint32_t mask;")
+        out.append(f'    asm("{sub_body(N)}"\n        : {outs}\n        : {ins});')
+        out.append("    return mask;")
+        out.append("}")
+        outs = ", ".join(f'"+r"(a[{i}])' for i in range(N))
+        ins = ", ".join(f'"r"(b[{i}])' for i in range(N - 1))
+        out.append(f"template <> __device__ __forceinline__ void mp_sub_hi<{W}>(uint32_t (&a)[{N}], "
+                   f"const uint32_t (&b)[{N}]) {{")
+        out.append(f'    asm("{sub_hi_body(W)}"\n        : {outs}\n        : {ins});')
         out.append("}")
     out.append("}  // namespace pm")
     print("\n".join(out))

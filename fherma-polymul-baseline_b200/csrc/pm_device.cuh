@@ -111,20 +111,35 @@ __device__ __forceinline__ int pass_index(int tid, int T, int m, int l, int logd
     return (blk << (logd + K)) + o + (l << logd);
 }
 
+// A pass index is a disjoint OR of thread bits (blk, o) and element bits (l),
+// and swz is linear over GF(2), so swz(idx) = swz(thread part) ^ swz(l << logd):
+// one XOR with a constant per access.
+template <int K>
+__device__ __forceinline__ int pass_thread_base(int tid, int T, int m, int logd) {
+    const int gid = tid + T * m;
+    const int blk = gid >> logd;
+    const int o = gid & ((1 << logd) - 1);
+    return swz((blk << (logd + K)) | o);
+}
+
 template <int K>
 __device__ __forceinline__ void pass_store(const uint32_t (&v)[8], uint32_t* s, int tid, int T, int logd) {
 #pragma unroll
-    for (int m = 0; m < (8 >> K); ++m)
+    for (int m = 0; m < (8 >> K); ++m) {
+        const int tb = pass_thread_base<K>(tid, T, m, logd);
 #pragma unroll
-        for (int l = 0; l < (1 << K); ++l) s[swz(pass_index<K>(tid, T, m, l, logd))] = v[(m << K) + l];
+        for (int l = 0; l < (1 << K); ++l) s[tb ^ swz(l << logd)] = v[(m << K) + l];
+    }
 }
 
 template <int K>
 __device__ __forceinline__ void pass_load(uint32_t (&v)[8], const uint32_t* s, int tid, int T, int logd) {
 #pragma unroll
-    for (int m = 0; m < (8 >> K); ++m)
+    for (int m = 0; m < (8 >> K); ++m) {
+        const int tb = pass_thread_base<K>(tid, T, m, logd);
 #pragma unroll
-        for (int l = 0; l < (1 << K); ++l) v[(m << K) + l] = s[swz(pass_index<K>(tid, T, m, l, logd))];
+        for (int l = 0; l < (1 << K); ++l) v[(m << K) + l] = s[tb ^ swz(l << logd)];
+    }
 }
 
 template <int K>
@@ -344,70 +359,60 @@ static __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeCons
 }
 
 // ---------------------------------------------------------------------------
-// Multiprecision tail of the CRT, per coefficient, all in registers.
-// v (W+2 words) mod q, v < 2^(sbits+37); q has sbits bits and W words;
+// Multiprecision tail of the CRT, per coefficient, all in registers, with the
+// carry-chain helpers of crt_mac.cuh.
+// v (W+2 words) mod q, v < 2^(sbits+37); q has sbits bits and at most W words
+// (W is its word count rounded up to a multiple of 4, so sbits > 32(W-4));
 // mu_q = floor(2^(sbits+62) / q).  Leaves the canonical residue in v[0..W).
 // ---------------------------------------------------------------------------
 template <int W>
 __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q, uint64_t mu_q,
                                              int sbits) {
-    // X = floor(v / 2^(sbits-1)), < 2^38
+    // X = floor(v / 2^(sbits-1)) < 2^38; only words W-4 .. W+1 can hold it
     const int sh = sbits - 1;
     uint64_t X = 0;
 #pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
+    for (int k = (W >= 4 ? W - 4 : 0); k < W + 2; ++k) {
         const int pos = 32 * k - sh;  // bit position of word k inside X
         if (pos > -32 && pos < 64) X |= pos >= 0 ? uint64_t(v[k]) << pos : uint64_t(v[k]) >> (-pos);
     }
+    // quotient estimate, at most 2 below floor(v / q)
     const uint64_t hi = __umul64hi(X, mu_q), lo = X * mu_q;
     const uint64_t Q = (hi << 1) | (lo >> 63);
-    const uint32_t qlo = uint32_t(Q), qhi = uint32_t(Q >> 32);
-    // v -= Q * q, computed as q*qlo + (q*qhi << 32)
-    uint32_t t[W + 2];
-    uint64_t c1 = 0, c2 = 0;
+    uint32_t qw[W];
 #pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
-        const uint64_t a1 = (k < W ? uint64_t(q[k]) * qlo : 0) + c1;
-        c1 = a1 >> 32;
-        const uint64_t a2 = (k >= 1 && k - 1 < W ? uint64_t(q[k - 1]) * qhi : 0) + uint32_t(a1) + c2;
-        c2 = a2 >> 32;
-        t[k] = uint32_t(a2);
-    }
-    uint32_t borrow = 0;
+    for (int k = 0; k < W; ++k) qw[k] = q[k];
+    uint32_t t[W + 2], u[W + 2];
 #pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
-        const uint64_t d = uint64_t(v[k]) - t[k] - borrow;
-        v[k] = uint32_t(d);
-        borrow = uint32_t(d >> 63);
-    }
-    // two conditional subtractions bring [0, 3q) to [0, q)
+    for (int k = 0; k < W + 2; ++k) t[k] = u[k] = 0;
+    crt_mac<W>(t, uint32_t(Q), qw);        // low 32 bits of Q times q
+    crt_mac<W>(u, uint32_t(Q >> 32), qw);  // high bits (< 2^6) times q, subtracted one word up
+    mp_sub<W + 2>(v, t);
+    mp_sub_hi<W>(v, u);
+    // [0, 3q) -> [0, q)
+    uint32_t qq[W + 2];
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) qq[k] = k < W ? qw[k] : 0u;
 #pragma unroll
     for (int rep = 0; rep < 2; ++rep) {
         uint32_t d[W + 2];
-        uint32_t br = 0;
 #pragma unroll
-        for (int k = 0; k < W + 2; ++k) {
-            const uint64_t x = uint64_t(v[k]) - (k < W ? q[k] : 0) - br;
-            d[k] = uint32_t(x);
-            br = uint32_t(x >> 63);
-        }
+        for (int k = 0; k < W + 2; ++k) d[k] = v[k];
+        const uint32_t borrowed = mp_sub<W + 2>(d, qq);
 #pragma unroll
-        for (int k = 0; k < W + 2; ++k) v[k] = br ? v[k] : d[k];
+        for (int k = 0; k < W + 2; ++k) v[k] = borrowed ? v[k] : d[k];
     }
 }
 
-// Final CRT step shared by the SIMT and tensor paths: v = acc + nearest *
+// Final CRT step shared by the SIMT and tensor paths: v += nearest *
 // (-P mod q), reduce mod q, store one coefficient (stride words).
 template <int W>
 __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t nearest, const uint32_t* s_q,
                                            uint64_t mu_q, int sbits, uint32_t* dst, int stride) {
-    uint32_t carry = 0;
+    uint32_t pneg[W];
 #pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
-        const uint64_t x = uint64_t(v[k]) + (k < W ? uint64_t(s_q[W + k]) * nearest : 0) + carry;
-        v[k] = uint32_t(x);
-        carry = uint32_t(x >> 32);
-    }
+    for (int k = 0; k < W; ++k) pneg[k] = s_q[W + k];
+    crt_mac<W>(v, nearest, pneg);
     reduce_mod_q<W>(v, s_q, mu_q, sbits);
 #pragma unroll
     for (int k = 0; k < W; k += 2)
