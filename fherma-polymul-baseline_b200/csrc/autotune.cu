@@ -6,6 +6,8 @@
 //                    register state, or fewer shared-memory exchanges);
 //   conv_ctas_per_sm persistent CTAs of the tensor conversion per SM;
 //   crt_ctas_per_sm  persistent CTAs of the tensor CRT per SM;
+//   row_persistent   K2 as one CTA per row, or as the persistent kernel that
+//                    stages each row's twiddles once per group and prefetches;
 //   group            products per launch group in batched calls (larger groups
 //                    fill the GPU, smaller ones keep residue planes in L2).
 // Coordinate descent from the defaults, objective = device time per product of
@@ -99,6 +101,11 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
             best = t;
         }
     };
+    if (s.logC >= 10) {
+        Tuning t = best;
+        t.row_persistent = !best.row_persistent;
+        consider(t);
+    }
     if (s.logC >= 4) {
         for (int radix : {2, 3}) {
             Tuning t = best;
@@ -148,6 +155,7 @@ extern "C" int pm_plan_autotune(pm_plan* plan, uint32_t reps, pm_tuning* chosen)
             chosen->conv_ctas_per_sm = uint32_t(t.conv_ctas_per_sm);
             chosen->crt_ctas_per_sm = uint32_t(t.crt_ctas_per_sm);
             chosen->group = t.group;
+            chosen->row_persistent = t.row_persistent ? 1u : 0u;
             chosen->us_per_product = us;
         }
         return PM_OK;
@@ -164,11 +172,13 @@ extern "C" int pm_plan_set_tuning(pm_plan* plan, const pm_tuning* t) {
     if (t->conv_ctas_per_sm < 1 || t->conv_ctas_per_sm > 8 || t->crt_ctas_per_sm < 1 || t->crt_ctas_per_sm > 4)
         return pm::fail(PM_ERR_INVALID, "CTAs per SM out of range");
     if (t->group > 64) return pm::fail(PM_ERR_INVALID, "group above 64");
+    if (t->row_persistent > 1) return pm::fail(PM_ERR_INVALID, "row_persistent must be 0 or 1");
     pm::Tuning& u = plan->core.tune;
     u.row_radix_log = t->row_radix == 4 ? 2 : 3;
     u.conv_ctas_per_sm = int(t->conv_ctas_per_sm);
     u.crt_ctas_per_sm = int(t->crt_ctas_per_sm);
     u.group = t->group;
+    u.row_persistent = t->row_persistent != 0;
     u.tuned = true;
     return PM_OK;
 }

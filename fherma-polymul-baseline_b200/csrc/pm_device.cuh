@@ -183,59 +183,17 @@ __device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, i
     }
 }
 
-constexpr int k2_threads(int logc) { return logc >= 12 ? 512 : (logc >= 11 ? 256 : 128); }
-constexpr int k2_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 3 : 7); }
-
-// Rows of C = 2^LOGC >= 8, passes of KP stages (radix 2^KP, KP = 2 or 3; the
-// last forward pass takes the remaining LOGC % KP stages).  grid
-// (R / rows_per_cta, P, count), block rows_per_cta * C/8.  Dynamic shared
-// memory per row: C uint2 forward and C uint2 inverse twiddles, then 2C words
-// of data.  The product overwrites the a plane in place.
-// One row r of prime i of the residue planes at `res` ([2][P][n]); the calling
-// CTA gives each row T = C/8 threads (sub = row slot in the CTA, tid = thread in
-// the row) and 24*C bytes of dynamic shared memory per row slot.
+// The forward row stages of a and b, the pointwise product and the inverse row
+// stages of one row, starting from the values a thread holds for the first pass
+// (pass_index<KP> with s0 = 0) and ending with the product in the same places.
+// sa, sb: 2C words of exchange space; stf, sti: the row's twiddles.
 template <int LOGC, int KP>
-__device__ __forceinline__ void k2_row_body(uint32_t* __restrict__ res, const PrimeConst& pc,
-                                            const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv,
-                                            int n, int logR, int P, int i, int r, int sub, int tid,
-                                            int rows_per_cta) {
+__device__ __forceinline__ void row_transform(uint32_t (&va)[8], uint32_t (&vb)[8], uint32_t* sa, uint32_t* sb,
+                                              const uint2* stf, const uint2* sti, int tid, const PrimeConst& pc) {
     constexpr int C = 1 << LOGC;
     constexpr int T = C / 8;
     constexpr int NP = LOGC / KP;   // full passes
     constexpr int REM = LOGC % KP;  // stages of the closing pass
-    static_assert(KP == 2 || KP == 3, "pass radix");
-    extern __shared__ uint2 smem2[];
-    const int R = 1 << logR;
-    uint2* stf = smem2 + sub * 2 * C;
-    uint2* sti = stf + C;
-    uint32_t* sa = reinterpret_cast<uint32_t*>(smem2 + rows_per_cta * 2 * C) + sub * 2 * C;
-    uint32_t* sb = sa + C;
-    uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
-    const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
-    constexpr int logd0 = LOGC - KP;  // first pass: s0 = 0
-
-    uint32_t va[8], vb[8];
-#pragma unroll
-    for (int m = 0; m < (8 >> KP); ++m)
-#pragma unroll
-        for (int l = 0; l < (1 << KP); ++l) {
-            const int idx = pass_index<KP>(tid, T, m, l, logd0);
-            va[(m << KP) + l] = ga[idx];
-            vb[(m << KP) + l] = gb[idx];
-        }
-    // this row's twiddles: local entry j = 2^s + i' holds Psi_rev[(R + r) 2^s + i']
-    {
-        const uint2* gf = tw_fwd + size_t(i) * kNMax;
-        const uint2* gi = tw_inv + size_t(i) * kNMax;
-        for (int j = tid; j < C; j += T) {
-            if (j == 0) continue;
-            const int s = 31 - __clz(j);
-            const int gidx = ((R + r) << s) + (j - (1 << s));
-            stf[j] = __ldg(gf + gidx);
-            sti[j] = __ldg(gi + gidx);
-        }
-    }
-    __syncthreads();
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
         const int s0 = KP * q, logd = LOGC - s0 - KP;
@@ -282,6 +240,60 @@ __device__ __forceinline__ void k2_row_body(uint32_t* __restrict__ res, const Pr
             __syncthreads();
         }
     }
+}
+
+constexpr int k2_threads(int logc) { return logc >= 12 ? 512 : (logc >= 11 ? 256 : 128); }
+constexpr int k2_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 3 : 7); }
+
+// Rows of C = 2^LOGC >= 8, passes of KP stages (radix 2^KP, KP = 2 or 3; the
+// last forward pass takes the remaining LOGC % KP stages).  grid
+// (R / rows_per_cta, P, count), block rows_per_cta * C/8.  Dynamic shared
+// memory per row: C uint2 forward and C uint2 inverse twiddles, then 2C words
+// of data.  The product overwrites the a plane in place.
+// One row r of prime i of the residue planes at `res` ([2][P][n]); the calling
+// CTA gives each row T = C/8 threads (sub = row slot in the CTA, tid = thread in
+// the row) and 24*C bytes of dynamic shared memory per row slot.
+template <int LOGC, int KP>
+__device__ __forceinline__ void k2_row_body(uint32_t* __restrict__ res, const PrimeConst& pc,
+                                            const uint2* __restrict__ tw_fwd, const uint2* __restrict__ tw_inv,
+                                            int n, int logR, int P, int i, int r, int sub, int tid,
+                                            int rows_per_cta) {
+    constexpr int C = 1 << LOGC;
+    constexpr int T = C / 8;
+    static_assert(KP == 2 || KP == 3, "pass radix");
+    extern __shared__ uint2 smem2[];
+    const int R = 1 << logR;
+    uint2* stf = smem2 + sub * 2 * C;
+    uint2* sti = stf + C;
+    uint32_t* sa = reinterpret_cast<uint32_t*>(smem2 + rows_per_cta * 2 * C) + sub * 2 * C;
+    uint32_t* sb = sa + C;
+    uint32_t* ga = res + size_t(i) * n + size_t(r) * C;
+    const uint32_t* gb = res + size_t(P + i) * n + size_t(r) * C;
+    constexpr int logd0 = LOGC - KP;  // first pass: s0 = 0
+
+    uint32_t va[8], vb[8];
+#pragma unroll
+    for (int m = 0; m < (8 >> KP); ++m)
+#pragma unroll
+        for (int l = 0; l < (1 << KP); ++l) {
+            const int idx = pass_index<KP>(tid, T, m, l, logd0);
+            va[(m << KP) + l] = ga[idx];
+            vb[(m << KP) + l] = gb[idx];
+        }
+    // this row's twiddles: local entry j = 2^s + i' holds Psi_rev[(R + r) 2^s + i']
+    {
+        const uint2* gf = tw_fwd + size_t(i) * kNMax;
+        const uint2* gi = tw_inv + size_t(i) * kNMax;
+        for (int j = tid; j < C; j += T) {
+            if (j == 0) continue;
+            const int s = 31 - __clz(j);
+            const int gidx = ((R + r) << s) + (j - (1 << s));
+            stf[j] = __ldg(gf + gidx);
+            sti[j] = __ldg(gi + gidx);
+        }
+    }
+    __syncthreads();
+    row_transform<LOGC, KP>(va, vb, sa, sb, stf, sti, tid, pc);
 #pragma unroll
     for (int m = 0; m < (8 >> KP); ++m)
 #pragma unroll

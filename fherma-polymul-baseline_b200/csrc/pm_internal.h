@@ -67,6 +67,7 @@ struct Tuning {
     int row_radix_log = 3;   // K2 register-pass radix: 2 (radix-4) or 3 (radix-8)
     int conv_ctas_per_sm = 4;  // K1T persistent CTAs per SM (per prime group share)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
+    bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)
     uint32_t group = 0;        // products per launch group in batches (0: fit ~64 MB of residues)
     bool tuned = false;
 };
@@ -74,6 +75,7 @@ struct Tuning {
 // Everything one (n, q) product needs on the device.
 struct PlanCore {
     int device = 0;
+    int sms = 148;           // streaming multiprocessors of the plan's device
     uint32_t n = 0, logn = 0, logR = 0, logC = 0;
     uint32_t P = 0;          // basis size
     uint32_t qbits = 0;

@@ -2,6 +2,7 @@
 // sequence of one product, and the C ABI declared in include/polymul.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,7 @@
 #include "host_math.h"
 #include "pm_device.cuh"
 #include "pm_internal.h"
+#include "rows_persistent.cuh"
 
 namespace pm {
 
@@ -257,6 +259,7 @@ PlanCore::~PlanCore() {
     cudaFree(d_scale);
     for (auto& sl : pipe) sl.reset();
     tensor_release(*this);
+    cudaFree(d_err);
     cudaFree(d_work);
     cudaFree(d_batch_work);
     cudaFree(d_io);
@@ -337,6 +340,10 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     cuda_check(cudaMemcpy(d_consts, consts.data(), consts.size() * 4, cudaMemcpyHostToDevice), "upload q");
     cuda_check(cudaMemcpy(d_scale, scale.data(), scale.size() * sizeof(uint2), cudaMemcpyHostToDevice),
                "upload CRT scales");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    if (sms <= 0) sms = 148;
+    cuda_check(cudaMalloc(&d_err, sizeof(uint32_t)), "allocate error word");
+    cuda_check(cudaMemset(d_err, 0, sizeof(uint32_t)), "clear error word");
     if (flags & PM_CONVERT_TENSOR) tensor_init(*this);
     if (tables_only) return;
     cuda_check(cudaMalloc(&d_work, workspace_bytes), "allocate residue workspace");
@@ -399,6 +406,22 @@ void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, const Batch
 template <int LOGC, int KP>
 void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
     constexpr int C = 1 << LOGC, T = C / 8;
+    if constexpr (LOGC >= 10) {
+        // bulk copies need 16-byte aligned rows (n, C and the product stride are multiples of 4 words)
+        if (s.tune.row_persistent && (reinterpret_cast<uintptr_t>(work) & 15) == 0 && (bt.ws_bstride & 3) == 0) {
+            const size_t smem = k2p_smem_bytes(LOGC);
+            cuda_check(cudaFuncSetAttribute(k2p_rows<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(smem)),
+                       "raise K2P shared memory");
+            const int64_t items = int64_t(s.P) << s.logR;
+            const int64_t total = items * bt.count;
+            const int ctas = int(std::min<int64_t>(total, int64_t(s.sms) * k2p_min_blocks(LOGC)));
+            k2p_rows<LOGC, KP><<<ctas, T, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
+                                                      int(s.n), int(s.logR), int(s.P), int(bt.count),
+                                                      bt.ws_bstride, s.d_err);
+            return;
+        }
+    }
     int rows = T >= 128 ? 1 : 128 / T;
     const int R = 1 << s.logR;
     if (rows > R) rows = R;

@@ -1,0 +1,146 @@
+// K2P: the row stages of K2 as a persistent kernel.
+//
+// Work items are (prime i, row r, product z) of one launch group, numbered
+// pair-major (pair = i * R + r, item = pair * count + z), so the items a CTA
+// takes in a row share their twiddles.  Each CTA owns a contiguous range of
+// items and, for each of them:
+//   - stages the pair's 2C forward/inverse row twiddles with bulk copies, only
+//     when the pair changes (once per pair instead of once per product);
+//   - has the item's two rows (a and b, 4C bytes each) in shared memory already:
+//     they were requested by bulk copy while the previous item was transformed;
+//   - requests the next item's rows into the other buffer, then runs the same
+//     register/shared-memory passes as K2 (row_transform) on this one, using
+//     its own data buffer as the exchange space, and stores the product row.
+// One row per CTA (T = C/8 threads), C >= 1024.  Bulk copies need 16-byte
+// aligned rows: the host launches this kernel only on 16-byte aligned
+// workspaces.
+//
+// Dynamic shared memory: C uint2 forward and C uint2 inverse twiddles, two data
+// buffers of 2C words, three mbarriers (data 0, data 1, twiddles): 32C + 24 B.
+#pragma once
+
+#include <cstdint>
+
+#include "pm_device.cuh"
+#include "tc_ptx.cuh"
+
+namespace pm {
+
+constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 3 : 6); }
+constexpr size_t k2p_smem_bytes(int logc) { return (size_t(32) << logc) + 3 * sizeof(uint64_t); }
+
+template <int LOGC, int KP>
+__global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
+    k2p_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
+             const uint2* __restrict__ tw_inv, int n, int logR, int P, int count, size_t ws_bstride,
+             uint32_t* __restrict__ err) {
+    constexpr int C = 1 << LOGC, T = C / 8;
+    constexpr int logd0 = LOGC - KP;  // first pass: s0 = 0
+    static_assert(LOGC >= 10, "one row per CTA needs C >= 1024");
+    extern __shared__ __align__(16) uint2 smem2[];
+    uint2* stf = smem2;
+    uint2* sti = smem2 + C;
+    uint32_t* sd = reinterpret_cast<uint32_t*>(smem2 + 2 * C);  // [2][2C] words
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sd + 4 * C);   // data 0, data 1, twiddles
+
+    const int tid = threadIdx.x;
+    const int R = 1 << logR;
+    const int total = P * R * count;
+    const int begin = int(int64_t(blockIdx.x) * total / gridDim.x);
+    const int end = int(int64_t(blockIdx.x + 1) * total / gridDim.x);
+    if (tid == 0) {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        tc::mbar_init(&bars[2], 1);
+    }
+    tc::fence_smem_async();
+    __syncthreads();
+
+    auto issue_rows = [&](int item, int buf) {
+        const int pair = item / count, z = item - pair * count;
+        const int i = pair >> logR, r = pair & (R - 1);
+        const uint32_t* src = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
+        uint32_t* dst = sd + buf * 2 * C;
+        tc::mbar_expect_tx(&bars[buf], 8u * C);
+        tc::bulk_load(dst, src, 4u * C, &bars[buf]);
+        tc::bulk_load(dst + C, src + size_t(P) * n, 4u * C, &bars[buf]);
+    };
+    // every thread tracks the copies: bit b of `phases` is the parity of barrier
+    // b's next completion, bit b of `pending` marks a copy not yet seen complete
+    uint32_t phases = 0, pending = 0;
+    bool ok = true;
+    auto wait = [&](int b) {
+        const bool done = tc::mbar_wait(&bars[b], (phases >> b) & 1u);
+        if (done) {
+            phases ^= 1u << b;
+            pending &= ~(1u << b);
+        }
+        ok = ok && done;
+    };
+    if (begin < end) {
+        if (tid == 0) issue_rows(begin, 0);
+        pending |= 1u;
+    }
+    int cur_pair = -1;
+    PrimeConst pc{};
+    for (int k = begin; k < end; ++k) {
+        const int buf = (k - begin) & 1;
+        const int pair = k / count, z = k - pair * count;
+        const int i = pair >> logR, r = pair & (R - 1);
+        if (k + 1 < end) {  // the other buffer's last reader was the previous item
+            if (tid == 0) issue_rows(k + 1, buf ^ 1);
+            pending |= 1u << (buf ^ 1);
+        }
+        if (pair != cur_pair) {  // twiddles are free: every thread passed the previous item's barrier
+            if (tid == 0) {
+                const uint2* gf = tw_fwd + size_t(i) * kNMax;
+                const uint2* gi = tw_inv + size_t(i) * kNMax;
+                // local entry j = 2^s + i' holds Psi_rev[(R + r) 2^s + i']; stage s > 0 is one
+                // contiguous, 16-byte aligned run of 2^s entries, stage 0 a single entry
+                tc::mbar_expect_tx(&bars[2], 16u * uint32_t(C - 2));
+                for (int s = 1; s < LOGC; ++s) {
+                    tc::bulk_load(stf + (1 << s), gf + (size_t(R + r) << s), 8u << s, &bars[2]);
+                    tc::bulk_load(sti + (1 << s), gi + (size_t(R + r) << s), 8u << s, &bars[2]);
+                }
+                stf[1] = __ldg(gf + R + r);
+                sti[1] = __ldg(gi + R + r);
+            }
+            pending |= 4u;
+            pc = pcs[i];
+            wait(2);
+            __syncthreads();  // entry 1, written by thread 0
+            cur_pair = pair;
+        }
+        wait(buf);
+
+        uint32_t* sa = sd + buf * 2 * C;
+        uint32_t* sb = sa + C;
+        uint32_t va[8], vb[8];
+#pragma unroll
+        for (int m = 0; m < (8 >> KP); ++m)
+#pragma unroll
+            for (int l = 0; l < (1 << KP); ++l) {
+                const int idx = pass_index<KP>(tid, T, m, l, logd0);
+                va[(m << KP) + l] = sa[idx];
+                vb[(m << KP) + l] = sb[idx];
+            }
+        row_transform<LOGC, KP>(va, vb, sa, sb, stf, sti, tid, pc);
+        uint32_t* ga = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
+#pragma unroll
+        for (int m = 0; m < (8 >> KP); ++m)
+#pragma unroll
+            for (int l = 0; l < (1 << KP); ++l) ga[pass_index<KP>(tid, T, m, l, logd0)] = va[(m << KP) + l];
+        // this thread's shared-memory writes are ordered before the next bulk copy into this buffer
+        tc::fence_smem_async();
+        if (__syncthreads_or(!ok)) break;
+    }
+    // after a wait gave up (and the loop stopped): copies already requested land
+    // before the CTA's shared memory goes away; no new copies were requested
+    if (tid == 0) {
+        for (int b = 0; b < 3; ++b)
+            if (pending & (1u << b)) tc::mbar_wait(&bars[b], (phases >> b) & 1u);
+        if (!ok) atomicOr(err, 1u);
+    }
+}
+
+}  // namespace pm

@@ -80,15 +80,11 @@ void tensor_init(PlanCore& s) {
     }
     cuda_check(cudaMalloc(&s.d_crt_weights, img.size()), "allocate CRT weights");
     cuda_check(cudaMemcpy(s.d_crt_weights, img.data(), img.size(), cudaMemcpyHostToDevice), "upload CRT weights");
-    cuda_check(cudaMalloc(&s.d_err, sizeof(uint32_t)), "allocate error word");
-    cuda_check(cudaMemset(s.d_err, 0, sizeof(uint32_t)), "clear error word");
 }
 
 void tensor_release(PlanCore& s) {
     cudaFree(s.d_crt_weights);
-    cudaFree(s.d_err);
     s.d_crt_weights = nullptr;
-    s.d_err = nullptr;
 }
 
 namespace {

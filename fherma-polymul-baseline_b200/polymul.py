@@ -45,7 +45,8 @@ class PlanInfo(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("row_radix", ctypes.c_uint32), ("conv_ctas_per_sm", ctypes.c_uint32),
-                ("crt_ctas_per_sm", ctypes.c_uint32), ("group", ctypes.c_uint32), ("us_per_product", ctypes.c_double)]
+                ("crt_ctas_per_sm", ctypes.c_uint32), ("group", ctypes.c_uint32), ("row_persistent", ctypes.c_uint32),
+                ("us_per_product", ctypes.c_double)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -204,8 +205,8 @@ class Plan:
         check(lib().pm_plan_autotune(self._h, reps, ctypes.byref(t)))
         return {name: getattr(t, name) for name, _ in Tuning._fields_}
 
-    def set_tuning(self, row_radix=8, conv_ctas_per_sm=4, crt_ctas_per_sm=2, group=0):
-        t = Tuning(row_radix, conv_ctas_per_sm, crt_ctas_per_sm, group, 0.0)
+    def set_tuning(self, row_radix=8, conv_ctas_per_sm=4, crt_ctas_per_sm=2, group=0, row_persistent=1):
+        t = Tuning(row_radix, conv_ctas_per_sm, crt_ctas_per_sm, group, row_persistent, 0.0)
         check(lib().pm_plan_set_tuning(self._h, ctypes.byref(t)))
 
     def multiply_host_batch(self, a, b, out=None):

@@ -203,7 +203,7 @@ def test_host_batch_pipeline(cuda, path, pinned):
         assert (got[k] == oracle.rns_multiply(a[k], b[k], q)).all()
 
 
-@pytest.mark.parametrize("n", [4096, 32768])
+@pytest.mark.parametrize("n", [4096, 16384, 32768, 65536])
 def test_tunings_do_not_change_results(cuda, path, n):
     """Every launch shape the autotuner may pick gives the same bits."""
     torch = cuda
@@ -214,14 +214,16 @@ def test_tunings_do_not_change_results(cuda, path, n):
     b = torch.from_numpy(np.stack([uniform_below(rng, q, n, 14) for _ in range(count)]).view(np.int64)).cuda()
     ref = None
     with make_plan(path, n, q, 14) as p:
-        for radix, conv, crt, group in [(8, 4, 2, 0), (4, 4, 2, 0), (8, 2, 1, 1), (4, 3, 1, 2), (8, 4, 2, 5)]:
-            p.set_tuning(radix, conv, crt, group)
+        shapes = [(8, 4, 2, 0, 1), (4, 4, 2, 0, 1), (8, 2, 1, 1, 1), (4, 3, 1, 2, 1), (8, 4, 2, 5, 1),
+                  (8, 4, 2, 0, 0), (4, 4, 2, 3, 0), (8, 4, 2, 3, 1)]
+        for radix, conv, crt, group, persistent in shapes:
+            p.set_tuning(radix, conv, crt, group, persistent)
             c = torch.zeros_like(a)
             p.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), count)
             torch.cuda.synchronize()
             if ref is None:
                 ref = c.clone()
-            assert torch.equal(c, ref), (radix, conv, crt, group)
+            assert torch.equal(c, ref), (radix, conv, crt, group, persistent)
         chosen = p.autotune()
         assert chosen["row_radix"] in (4, 8) and chosen["us_per_product"] > 0
         c = torch.zeros_like(a)
