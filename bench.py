@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default launch shapes instead of the autotuner's")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="K",
-                    help="no timing: run K single products (one launch sequence each) for an ncu capture")
+                    help="no timing: one batched call of K products in one launch group (one launch per pass), "
+                         "for an ncu capture")
     return ap.parse_args()
 
 
@@ -430,6 +431,26 @@ def read_profile_traffic(kernel):
     return None
 
 
+def pcie_bandwidth(torch, device, nbytes=256 << 20, reps=4):
+    """Pinned host <-> device copy rates (GB/s), each direction alone, CUDA events on a side stream."""
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
+    st = torch.cuda.Stream()
+    out = {}
+    for name, dst, src in (("h2d_gbs", d, h), ("d2h_gbs", h, d)):
+        with torch.cuda.stream(st):
+            dst.copy_(src, non_blocking=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(reps):
+                dst.copy_(src, non_blocking=True)
+            e1.record(st)
+        e1.synchronize()
+        out[name] = reps * nbytes / (e0.elapsed_time(e1) / 1000.0) / 1e9
+    del h, d
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -524,6 +545,11 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, world, "cuda")
     e2e_value = E * args.steps * world / e2e_s
     io = n * 8 * limbs
+    link = pcie_bandwidth(torch, local)
+    # the copies bound the host-buffer call: 2 polynomials in and 1 out per product, the two
+    # directions on separate copy engines
+    link["bound_products_per_s"] = 1.0 / max(2 * io / (link["h2d_gbs"] * 1e9), io / (link["d2h_gbs"] * 1e9))
+    link["frac"] = e2e_value / world / link["bound_products_per_s"]
 
     # roofline of the dominant kernel
     alg = algorithmic_bytes(n, plan.primes, limbs)
@@ -602,7 +628,8 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}", "oracle_check": f"{checked} products bit-exact",
                        "tuning": tuning},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * E * io, "d2h_bytes_per_step": E * io,
-                    "api": "pm_multiply_host_batch, pinned host buffers", "products_per_step": E},
+                    "api": "pm_multiply_host_batch, pinned host buffers", "products_per_step": E,
+                    "link": link},
             "gpu_launches": launches,
             "roofline": roofline,
             "alu_roofline": alu,
@@ -633,7 +660,8 @@ def run_ncu_case(args):
     b = device_inputs(torch, args.ncu_case, args.ring, limbs, q, args.seed + 29)
     c = torch.empty_like(a)
     plan = polymul.Plan(args.ring, q, coef_limbs=limbs, tensor=(args.path == "tensor"))
-    # one batched call: the products go through the passes in launch groups, as in the timed step
+    # one batched call, all K products in one launch group (one launch per pass)
+    plan.set_tuning(group=args.ncu_case)
     plan.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), args.ncu_case)
     torch.cuda.synchronize()
     plan.close()

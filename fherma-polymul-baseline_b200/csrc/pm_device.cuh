@@ -426,6 +426,13 @@ __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t neares
     for (int k = 0; k < W; ++k) pneg[k] = s_q[W + k];
     crt_mac<W>(v, nearest, pneg);
     reduce_mod_q<W>(v, s_q, mu_q, sbits);
+    if ((stride & 3) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+#pragma unroll
+        for (int k = 0; k < W; k += 4)
+            if (k < stride) *reinterpret_cast<uint4*>(dst + k) = make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+        for (int k = W; k < stride; k += 4) *reinterpret_cast<uint4*>(dst + k) = make_uint4(0, 0, 0, 0);
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < W; k += 2)
         if (k < stride) *reinterpret_cast<uint2*>(dst + k) = make_uint2(v[k], v[k + 1]);

@@ -618,7 +618,11 @@ void PlanCore::ensure_pipeline(uint32_t group) {
 
 void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count) {
     if (!count) return;
-    uint32_t g = group_size(s);
+    // Chunks of at most kHostChunk products: the copies, not the kernels, bound
+    // this call (a chunk's kernels take a fraction of its H2D time), so small
+    // chunks shorten the pipeline's fill and drain.
+    constexpr uint32_t kHostChunk = 4;
+    uint32_t g = std::min(group_size(s), kHostChunk);
     if (g > count) g = count;
     s.ensure_pipeline(g);
     auto pinned = [](const void* p) {

@@ -134,12 +134,13 @@ CUtensorMap coefficient_map(const PlanCore& s, const void* base, uint32_t count)
     return make_map(CU_TENSOR_MAP_DATA_TYPE_UINT8, base, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
-// the product planes (plane 0..P-1) of `count` workspaces: dims (column, row, prime, product)
+// the product planes (plane 0..P-1) of `count` workspaces: dims (column, prime, row, product),
+// so a box lands in shared memory as [row][prime][column]
 CUtensorMap residue_map(const PlanCore& s, const void* work, uint32_t count) {
     const uint32_t C = 1u << s.logC, R = 1u << s.logR, Gc = C < 8 ? C : 8;
-    const cuuint64_t dims[4] = {C, R, s.P, count};
-    const cuuint64_t strides[3] = {C * 4ull, C * R * 4ull, s.workspace_bytes};
-    const cuuint32_t box[4] = {Gc, R, s.P, 1};
+    const cuuint64_t dims[4] = {C, s.P, R, count};
+    const cuuint64_t strides[3] = {C * R * 4ull, C * 4ull, s.workspace_bytes};
+    const cuuint32_t box[4] = {Gc, s.P, R, 1};
     return make_map(CU_TENSOR_MAP_DATA_TYPE_UINT32, work, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE);
 }
 

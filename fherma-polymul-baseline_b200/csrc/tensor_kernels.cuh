@@ -78,12 +78,14 @@ struct PlanConvWork {
     uint32_t* work;
     size_t ws_bstride;
     int n, logC, P, count, pgs;
-    __device__ int groups() const { return (1 << logC) / min(1 << logC, 8); }
-    __device__ int total() const { return pgs * count * 2 * groups(); }
+    // column groups per row: C / min(C, 8) = 2^lg, lg = logC - min(logC, 3)
+    __device__ int lg() const { return logC - min(logC, 3); }
+    __device__ int total() const { return pgs * (count << (lg() + 1)); }
     __device__ ConvItem item(int k) const {
-        const int per_pg = count * 2 * groups();
+        const int g = lg();
+        const int per_pg = count << (g + 1);
         const int pg = k / per_pg, rest = k - pg * per_pg;
-        return ConvItem{rest / (2 * groups()), pg, (rest / groups()) & 1, rest % groups()};
+        return ConvItem{rest >> (g + 1), pg, (rest >> g) & 1, rest & ((1 << g) - 1)};
     }
     __device__ ConvTarget target(int z, int poly) const {
         return ConvTarget{poly ? &map_b : &map_a, z, work + z * ws_bstride, n, logC, P};
@@ -117,9 +119,9 @@ struct PlanCrtWork {
     const uint8_t* crt_w;
     uint64_t mu_q;
     int sbits, n, logC, P, stride, count, use_tma;
-    __device__ int groups() const { return (1 << logC) / min(1 << logC, 8); }
-    __device__ int total() const { return count * groups(); }
-    __device__ int2 item(int k) const { return make_int2(k / groups(), k % groups()); }
+    __device__ int lg() const { return logC - min(logC, 3); }  // column groups per row = 2^lg
+    __device__ int total() const { return count << lg(); }
+    __device__ int2 item(int k) const { return make_int2(k >> lg(), k & ((1 << lg()) - 1)); }
     __device__ CrtTarget target(int z) const {
         return CrtTarget{&map_res, z, work + z * ws_bstride, out + z * io_bstride, scale, consts, crt_w, mu_q,
                          sbits, n, logC, P, stride, use_tma};
@@ -149,12 +151,19 @@ struct TableCrtWork {
 // K1T: tensor-core conversion + forward column stages, persistent.  Block 128.
 // A tile holds coefficient r*C + Gc*cg + c of one polynomial in row m = r*Gc + c
 // and arrives by TMA (box: 128 bytes x Gc columns x R rows, 128-byte swizzle,
-// bytes past the coefficient width zero-filled), double-buffered so the next
-// item loads while this one is converted.  Items are ordered prime group
+// bytes past the coefficient width zero-filled).  Items are ordered prime group
 // first; the group's pre-swizzled weights (B), constants and column twiddles
 // are reloaded when the group changes.
-// Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose 16x128 words.
+// Pipeline per CTA: two A tiles and two TMEM accumulators (64 columns each).
+// While the epilogue of item k reads accumulator k%2, the MMA of item k+1
+// (same prime group) already runs into the other one, and the TMA of item k+2
+// fills the A tile item k's MMA has finished reading.
+// Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose
+// 16 x kTS words (kTS = 136: the four primes a warp reads per row sit 8 banks
+// apart).
 // ---------------------------------------------------------------------------
+constexpr int kTS = 136;
+
 template <int LOGR, class Work>
 __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work w,
                                                    const PrimeConst* __restrict__ pcs,
@@ -165,8 +174,8 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = sbase;                        // 2 x (128 x 128 B)
     uint8_t* sB = sbase + 32768;                // 64 x 128 B
-    uint32_t* sT = reinterpret_cast<uint32_t*>(sbase + 32768 + 8192);  // [16][128] residues
-    __shared__ uint64_t tma_bar[2], mma_bar;
+    uint32_t* sT = reinterpret_cast<uint32_t*>(sbase + 32768 + 8192);  // [16][kTS] residues
+    __shared__ uint64_t tma_bar[2], mma_bar[2];
     __shared__ uint32_t tmem_base;
     __shared__ PrimeConst spc[tc::kConvGroup];
 
@@ -177,11 +186,12 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
     const int end = min(total, begin + chunk);
 
     for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
-    if (warp == 0) tc::tmem_alloc(&tmem_base, 64);
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
     if (tid == 0) {
         tc::mbar_init(&tma_bar[0], 1);
         tc::mbar_init(&tma_bar[1], 1);
-        tc::mbar_init(&mma_bar, 1);
+        tc::mbar_init(&mma_bar[0], 1);
+        tc::mbar_init(&mma_bar[1], 1);
     }
     tc::fence_smem_async();
     tc::fence_before();
@@ -197,7 +207,26 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
         tc::mbar_expect_tx(&tma_bar[buf], 128u * uint32_t(Gc) * uint32_t(R));
         tc::tma_load_4d(sA + buf * 16384, t.map, 0, it.cg * Gc, 0, t.mz, &tma_bar[buf]);
     };
-    if (tid == 0 && begin < end) issue(begin, 0);
+    // thread 0 only: bit b = parity of A tile b's next TMA completion
+    uint32_t tma_phases = 0;
+    bool ok = true;
+    // thread 0: the item in A tile `buf` times B into accumulator `buf`
+    auto mma = [&](int buf) {
+        ok = tc::mbar_wait(&tma_bar[buf], (tma_phases >> buf) & 1u) && ok;
+        tma_phases ^= 1u << buf;
+        tc::fence_after();
+        const uint32_t a0 = tc::smem_u32(sA + buf * 16384), b0 = tc::smem_u32(sB);
+        constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kConvN);
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks)
+            tc::mma_u8(tbase + 64 * buf, tc::sw128_desc(a0 + 32 * ks), tc::sw128_desc(b0 + 32 * ks), idesc,
+                       ks > 0);
+        tc::mma_commit(&mma_bar[buf]);
+    };
+    if (tid == 0) {
+        if (begin < end) issue(begin, 0);
+        if (begin + 1 < end) issue(begin + 1, 1);
+    }
 
     // column-stage role: prime j of the group, column c of the tile
     const int cj = tid / 8, cc = tid % 8;
@@ -205,14 +234,15 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
     PrimeConst cpc{};
     int cur_pg = -1;
 
-    uint32_t tma_phases = 0, mma_phase = 0;  // bit b: parity of buffer b's next TMA completion
-    bool ok = true;
+    uint32_t mma_phases = 0;  // bit b: parity of accumulator b's next MMA completion
     int kk = 0;
     for (int k = begin; k < end; ++k, ++kk) {
         const ConvItem it = w.item(k);
         const ConvTarget t = w.target(it.z, it.poly);
         const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
-        if (it.pg != cur_pg) {  // all earlier MMAs are complete: B may be rewritten
+        const int buf = kk & 1;
+        if (it.pg != cur_pg) {
+            // every MMA issued so far is complete and none reads B for this item yet: B may be rewritten
             const uint4* src = reinterpret_cast<const uint4*>(conv_w + size_t(it.pg) * 8192);
             for (int q = tid; q < 512; q += 128) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
             if (tid < tc::kConvGroup) spc[tid] = pcs[it.pg * tc::kConvGroup + tid];
@@ -223,37 +253,34 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
             cur_pg = it.pg;
             tc::fence_smem_async();
             __syncthreads();
+            if (tid == 0) mma(buf);
         }
         const int np = min(tc::kConvGroup, t.P - it.pg * tc::kConvGroup);
-        const int buf = kk & 1;
-        if (tid == 0) {
-            ok = tc::mbar_wait(&tma_bar[buf], (tma_phases >> buf) & 1u) && ok;
-            tc::fence_after();
-            const uint32_t a0 = tc::smem_u32(sA + buf * 16384), b0 = tc::smem_u32(sB);
-            constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kConvN);
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks)
-                tc::mma_u8(tbase, tc::sw128_desc(a0 + 32 * ks), tc::sw128_desc(b0 + 32 * ks), idesc, ks > 0);
-            tc::mma_commit(&mma_bar);
-            // the other buffer's last reader was the previous item's MMA, already complete
-            if (k + 1 < end) issue(k + 1, buf ^ 1);
-        }
-        tma_phases ^= 1u << buf;
-        ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
-        mma_phase ^= 1;
+        ok = tc::mbar_wait(&mma_bar[buf], (mma_phases >> buf) & 1u) && ok;
+        mma_phases ^= 1u << buf;
         tc::fence_after();
+        if (tid == 0) {
+            // this item's MMA has read A tile `buf`: load item k+2 into it
+            if (k + 2 < end) issue(k + 2, buf);
+            // the next item's MMA runs during this epilogue (its accumulator was
+            // drained before the previous item's closing barrier)
+            if (k + 1 < end && w.item(k + 1).pg == cur_pg) mma(buf ^ 1);
+        }
         // --- residues of row m = tid for the group's 16 primes ---
+        // byte-plane sums d_a <= 128 * 255^2 < 2^23, so d0 + 2^8 d1 and d2 + 2^8 d3
+        // fit 32 bits and the residue input is (d2 + 2^8 d3) 2^16 + d0 + 2^8 d1 < 2^48
 #pragma unroll
         for (int q4 = 0; q4 < 4; ++q4) {
             uint32_t d[16];
-            tc::tmem_ld16(taddr + 16 * q4, d);
+            tc::tmem_ld16(taddr + 64 * buf + 16 * q4, d);
             tc::tmem_wait_ld();
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int j = 4 * q4 + u;
-                const uint64_t v = uint64_t(d[4 * u]) + (uint64_t(d[4 * u + 1]) << 8) +
-                                   (uint64_t(d[4 * u + 2]) << 16) + (uint64_t(d[4 * u + 3]) << 24);
-                sT[j * 128 + tid] = reduce60(v, spc[j].p, spc[j].mu);
+                const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
+                const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
+                const uint64_t v = (uint64_t(hi) << 16) + lo;
+                sT[j * kTS + tid] = reduce60(v, spc[j].p, spc[j].mu);
             }
         }
         tc::fence_before();
@@ -263,7 +290,7 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
             const int ci = it.pg * tc::kConvGroup + cj;
             uint32_t v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = sT[cj * 128 + r * Gc + cc];
+            for (int r = 0; r < R; ++r) v[r] = sT[cj * kTS + r * Gc + cc];
 #pragma unroll
             for (int s = 0; s < LOGR; ++s) {
                 const int h = R >> (s + 1);
@@ -281,16 +308,20 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
-        tc::tmem_dealloc(tbase, 64);
+        tc::tmem_dealloc(tbase, 128);
     }
     if (!ok && tid == 0) atomicOr(err, 1u);
 }
 
 // ---------------------------------------------------------------------------
 // K3T: inverse column stages + CRT on the tensor cores, persistent.  Block 128.
-// An item's residues for every prime arrive by TMA (box: Gc columns x R rows x
-// P primes of u32); the next item's box is requested as soon as this one has
-// been turned into CRT digits, so it loads during the MMA and the epilogue.
+// An item's residues for every prime arrive by TMA (box: Gc columns x P primes x
+// R rows of u32, landing as [row][prime][column], so the 4 primes x 8 columns a
+// warp reads per row fall in 32 distinct banks); the next item's box is
+// requested as soon as this one has been turned into CRT digits, so it loads
+// during the MMA and the epilogue.  A-tile row m = r*Gc + c holds the digits of
+// coefficient (row r, column c): a warp's digit stores (8 columns x 4 primes)
+// then also hit 32 distinct banks of the 128-byte swizzle.
 // The CRT weights, q constants and column twiddles of the current product stay
 // in shared memory until an item of another product needs its own.
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB,
@@ -306,7 +337,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = sbase;                                        // [2][128][128 B]
     uint8_t* sB = sbase + 32768;                                // [2][128][128 B]
-    uint32_t* sR = reinterpret_cast<uint32_t*>(sbase + 65536);  // [P][R][Gc]
+    uint32_t* sR = reinterpret_cast<uint32_t*>(sbase + 65536);  // [R][P][Gc]
     uint2* sTw = reinterpret_cast<uint2*>(sR + tc::kMaxPrimes * R * 8);  // [P][R-1]
     __shared__ uint64_t tma_bar, mma_bar;
     __shared__ uint32_t tmem_base;
@@ -370,7 +401,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         } else {
             const int box = t.P * R * Gc;
             for (int q = tid; q < box; q += 128) {
-                const int c = q % Gc, r = (q / Gc) % R, i = q / (Gc * R);
+                const int c = q % Gc, i = (q / Gc) % t.P, r = q / (Gc * t.P);
                 sR[q] = t.work[size_t(i) * t.n + (size_t(r) << t.logC) + size_t(cg) * Gc + c];
             }
             __syncthreads();
@@ -382,7 +413,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
             const PrimeConst pc = pcs[i];
             uint32_t v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = sR[(i * R + r) * Gc + c];
+            for (int r = 0; r < R; ++r) v[r] = sR[(r * t.P + i) * Gc + c];
             const uint2* tw = sTw + i * RT - 1;  // tw[k] = Psi_inv_rev[k], k >= 1
 #pragma unroll
             for (int s = LOGR - 1; s >= 0; --s) {
@@ -396,7 +427,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const uint32_t x = csub(shoup_mul(v[r], sc, pc.p), pc.p);
-                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(c * R + r, kb)) = x;
+                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(r * Gc + c, kb)) = x;
             }
         }
         tc::fence_smem_async();
@@ -448,8 +479,8 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         const uint64_t f1 = fsum1 + (fsum0 >> 32);
         // nearest integer of sum t_i / p_i: (f1 * 2^32 + low) / 2^64 rounded
         const uint32_t nearest = uint32_t(f1 >> 32) + (uint32_t(f1) >> 31);
-        const int cc = tid / R, rr = tid % R;
-        if (cc < Gc) {
+        const int rr = tid / Gc, cc = tid % Gc;
+        if (rr < R) {
             const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
             crt_finish<W>(acc, nearest, s_q, t.mu_q, t.sbits, t.out + J * t.stride, t.stride);
         }
@@ -464,7 +495,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
 }
 
 // shared-memory bytes the kernels above ask for
-constexpr size_t k1t_smem_bytes() { return 1024 + 32768 + 8192 + 16 * 128 * 4; }
+constexpr size_t k1t_smem_bytes() { return 1024 + 32768 + 8192 + 16 * kTS * 4; }
 template <int LOGR>
 constexpr size_t k3t_smem_bytes() {
     return 1024 + 65536 + size_t(tc::kMaxPrimes) * (1 << LOGR) * 8 * 4 +
