@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--uneven", type=int, default=64, help="products in the uneven batch (0 skips it)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default launch shapes instead of the autotuner's")
+    ap.add_argument("--group", type=int, default=0,
+                    help="products per launch group (default launch shapes otherwise; skips the autotuner)")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="K",
                     help="no timing: one batched call of K products in one launch group (one launch per pass), "
                          "for an ncu capture")
@@ -464,7 +466,12 @@ def run_ours(args):
     q = seeded_q(args.seed, bits)
     limbs = (bits + 63) // 64
     plan = polymul.Plan(n, q, coef_limbs=limbs, tensor=(args.path == "tensor"))
-    tuning = plan.autotune(reps=3) if args.autotune else None
+    tuning = None
+    if args.group:
+        plan.set_tuning(group=args.group)
+        tuning = {"group": args.group, "source": "--group"}
+    elif args.autotune:
+        tuning = plan.autotune(reps=3)
     B = args.batch
     A = device_inputs(torch, B, n, limbs, q, args.seed + 17 + 1000 * rank)
     Bv = device_inputs(torch, B, n, limbs, q, args.seed + 29 + 1000 * rank)

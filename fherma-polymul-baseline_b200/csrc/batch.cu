@@ -192,7 +192,7 @@ struct BatchCore {
         const DeviceBasis& B = *plans[0]->basis;
         const int sms = sm_count_dev();
         TableConvWork cw{d_conv_items, conv_items, d_prod, d_maps, d_work};
-        k1t_convert<4, TableConvWork><<<std::min(conv_items, sms * conv_ctas_per_sm), 128, k1t_smem_bytes(), st0>>>(
+        k1t_convert<4, TableConvWork><<<std::min(conv_items, sms * conv_ctas_per_sm), tc::kConvThreads, k1t_smem_bytes(), st0>>>(
             cw, B.d_pc, B.d_conv_weights, B.d_tw_fwd, d_err);
         cuda_check(cudaGetLastError(), "batch conversion launch");
         auto fork = [&](size_t k) {

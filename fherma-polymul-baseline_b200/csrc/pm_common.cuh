@@ -16,7 +16,7 @@ struct PrimeConst {
     uint32_t p;
     uint32_t two_p;
     uint32_t mu;    // floor(2^61 / p), p in (2^29, 2^30)
-    uint32_t pad;
+    uint32_t pinv;  // p^-1 mod 2^32 (Montgomery reduction)
     uint64_t recip; // floor(2^64 / p)
 };
 
@@ -36,6 +36,15 @@ __device__ __forceinline__ uint32_t reduce60(uint64_t x, uint32_t p, uint32_t mu
     uint32_t r = uint32_t(x) - q * p;
     r = csub(r, p);
     return csub(r, p);
+}
+
+// x * y * 2^-32 mod p up to one extra p, for x, y in [0, 2p): result in (0, 2p).
+// Montgomery reduction with m = lo(xy) p^-1: xy - m p is a multiple of 2^32 and,
+// as xy < 4p^2 < p 2^32, (xy - m p) / 2^32 lies in (-p, p).
+__device__ __forceinline__ uint32_t mont_mul(uint32_t x, uint32_t y, uint32_t p, uint32_t pinv) {
+    const uint64_t t = uint64_t(x) * y;
+    const uint32_t m = uint32_t(t) * pinv;
+    return uint32_t(t >> 32) - __umulhi(m, p) + p;
 }
 
 // Forward Cooley-Tukey butterfly, Harvey lazy: x, y in [0, 4p) -> [0, 4p).

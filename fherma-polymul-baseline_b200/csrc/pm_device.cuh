@@ -215,13 +215,10 @@ __device__ __forceinline__ void row_transform(uint32_t (&va)[8], uint32_t (&vb)[
         pass_load<REM>(vb, sb, tid, T, logd);
         pass_forward<REM>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
     }
-    // pointwise product, operands reduced to [0, p)
+    // pointwise product in Montgomery form (a factor 2^-32 the CRT scale removes), in [0, 2p)
 #pragma unroll
-    for (int l = 0; l < 8; ++l) {
-        const uint32_t x = csub(csub(va[l], pc.two_p), pc.p);
-        const uint32_t y = csub(csub(vb[l], pc.two_p), pc.p);
-        va[l] = reduce60(uint64_t(x) * y, pc.p, pc.mu);
-    }
+    for (int l = 0; l < 8; ++l)
+        va[l] = mont_mul(csub(va[l], pc.two_p), csub(vb[l], pc.two_p), pc.p, pc.pinv);
     if constexpr (REM > 0) {
         const int s0 = KP * NP, logd = 0;
         pass_inverse<REM>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
@@ -349,11 +346,7 @@ static __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeCons
             }
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const uint32_t x = csub(csub(va[j], pc.two_p), pc.p);
-        const uint32_t y = csub(csub(vb[j], pc.two_p), pc.p);
-        va[j] = reduce60(uint64_t(x) * y, pc.p, pc.mu);
-    }
+    for (int j = 0; j < 4; ++j) va[j] = mont_mul(csub(va[j], pc.two_p), csub(vb[j], pc.two_p), pc.p, pc.pinv);
     for (int s = logC - 1; s >= 0; --s) {
         const int t = C >> (s + 1);
 #pragma unroll

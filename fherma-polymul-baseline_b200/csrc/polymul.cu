@@ -202,7 +202,9 @@ DeviceBasis& basis_for_device(int device) {
             pc[i].p = p;
             pc[i].two_p = 2 * p;
             pc[i].mu = uint32_t((uint64_t(1) << 61) / p);
-            pc[i].pad = 0;
+            uint32_t pinv = p;  // p^-1 mod 2^32 by Newton: p * p = 1 mod 8, each step doubles the bits
+            for (int it = 0; it < 5; ++it) pinv *= 2u - p * pinv;
+            pc[i].pinv = pinv;
             pc[i].recip = uint64_t(((unsigned __int128)1 << 64) / p);
         }
     };
@@ -302,7 +304,8 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     basis = &basis_for_device(device);
     P = basis_size(basis->primes, n, qbits);
 
-    // CRT constants: (P_total / p_i) mod q, (-P_total) mod q, scale = n^-1 (P/p_i)^-1 mod p_i
+    // CRT constants: (P_total / p_i) mod q, (-P_total) mod q,
+    // scale = 2^32 n^-1 (P/p_i)^-1 mod p_i (2^32 undoes the Montgomery product of K2)
     Words total{1};
     for (unsigned i = 0; i < P; ++i) total = multiply_small(total, basis->primes[i]);
     std::vector<uint32_t> mq(size_t(P) * W, 0), consts(2 * size_t(W), 0);
@@ -315,7 +318,8 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
         std::copy(mmod.begin(), mmod.end(), mq.begin() + size_t(i) * W);
         const uint32_t minv = powmod(mod_small(m, p), p - 2, p);
         const uint32_t ninv = powmod(n % p, p - 2, p);
-        const uint32_t s = mulmod(minv, ninv, p);
+        const uint32_t r32 = uint32_t((uint64_t(1) << 32) % p);
+        const uint32_t s = mulmod(mulmod(minv, ninv, p), r32, p);
         scale[i] = make_uint2(s, shoup_of(s, p));
     }
     const Words qpad = padded(q, W);

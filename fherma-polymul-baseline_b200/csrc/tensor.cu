@@ -167,7 +167,7 @@ void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
     w.P = int(s.P);
     w.count = int(count);
     w.pgs = pgs;
-    k1t_convert<LOGR, PlanConvWork><<<ctas, 128, smem, st>>>(w, s.basis->d_pc, s.basis->d_conv_weights,
+    k1t_convert<LOGR, PlanConvWork><<<ctas, tc::kConvThreads, smem, st>>>(w, s.basis->d_pc, s.basis->d_conv_weights,
                                                              s.basis->d_tw_fwd, s.d_err);
 }
 

@@ -148,161 +148,212 @@ struct TableCrtWork {
 };
 
 // ---------------------------------------------------------------------------
-// K1T: tensor-core conversion + forward column stages, persistent.  Block 128.
+// K1T: tensor-core conversion + forward column stages, persistent and warp
+// specialised.  Block kConvThreads = 160: warps 0-3 are the workers (epilogue
+// and column stages, one coefficient row per thread), warp 4 the producer.
 // A tile holds coefficient r*C + Gc*cg + c of one polynomial in row m = r*Gc + c
 // and arrives by TMA (box: 128 bytes x Gc columns x R rows, 128-byte swizzle,
 // bytes past the coefficient width zero-filled).  Items are ordered prime group
-// first; the group's pre-swizzled weights (B), constants and column twiddles
-// are reloaded when the group changes.
-// Pipeline per CTA: two A tiles and two TMEM accumulators (64 columns each).
-// While the epilogue of item k reads accumulator k%2, the MMA of item k+1
-// (same prime group) already runs into the other one, and the TMA of item k+2
-// fills the A tile item k's MMA has finished reading.
+// first.
+// Producer (one lane issues): B (the group's pre-swizzled weights, 8 KB) by bulk
+// copy when the group changes; per item: wait for its A tile, wait until the
+// workers have drained the accumulator it reuses, four tcgen05.mma (M=128,
+// N=64, K=32) into that accumulator, commit; once the MMA is complete its A tile
+// takes the TMA of the item two ahead.
+// Workers: wait for the item's MMA, tcgen05.ld -> two 32-bit partial sums ->
+// Barrett -> padded transpose, release the accumulator (mbarrier arrival), then
+// 4 forward column stages in registers -> residue planes.  Only the workers
+// meet at (named) barriers, so the producer's waits never hold them.
+// Barriers: tma_full[2], mma_full[2], tmem_empty[2] (128 arrivals), b_full.
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose
 // 16 x kTS words (kTS = 136: the four primes a warp reads per row sit 8 banks
-// apart).
+// apart).  TMEM: 2 x 64 columns.
 // ---------------------------------------------------------------------------
 constexpr int kTS = 136;
+namespace tc {
+constexpr int kConvThreads = 160;
+}
 
 template <int LOGR, class Work>
-__global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work w,
-                                                   const PrimeConst* __restrict__ pcs,
-                                                   const uint8_t* __restrict__ conv_w,
-                                                   const uint2* __restrict__ tw_fwd, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_constant__ Work w,
+                                                                const PrimeConst* __restrict__ pcs,
+                                                                const uint8_t* __restrict__ conv_w,
+                                                                const uint2* __restrict__ tw_fwd,
+                                                                uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = sbase;                        // 2 x (128 x 128 B)
     uint8_t* sB = sbase + 32768;                // 64 x 128 B
     uint32_t* sT = reinterpret_cast<uint32_t*>(sbase + 32768 + 8192);  // [16][kTS] residues
-    __shared__ uint64_t tma_bar[2], mma_bar[2];
+    __shared__ uint64_t tma_full[2], mma_full[2], tmem_empty[2], b_full;
     __shared__ uint32_t tmem_base;
+    __shared__ volatile uint32_t s_abort;
     __shared__ PrimeConst spc[tc::kConvGroup];
 
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int total = w.total();
     const int chunk = (total + int(gridDim.x) - 1) / int(gridDim.x);
     const int begin = int(blockIdx.x) * chunk;
     const int end = min(total, begin + chunk);
 
-    for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
+    for (int k = tid; k < 2048; k += tc::kConvThreads) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
     if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
     if (tid == 0) {
-        tc::mbar_init(&tma_bar[0], 1);
-        tc::mbar_init(&tma_bar[1], 1);
-        tc::mbar_init(&mma_bar[0], 1);
-        tc::mbar_init(&mma_bar[1], 1);
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&tma_full[b], 1);
+            tc::mbar_init(&mma_full[b], 1);
+            tc::mbar_init(&tmem_empty[b], 128);
+        }
+        tc::mbar_init(&b_full, 1);
+        s_abort = 0;
     }
     tc::fence_smem_async();
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     const uint32_t tbase = tmem_base;
-    const uint32_t taddr = tbase + (uint32_t(32 * (warp & 3)) << 16);
-
-    auto issue = [&](int k, int buf) {
-        const ConvItem it = w.item(k);
-        const ConvTarget t = w.target(it.z, it.poly);
-        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
-        tc::mbar_expect_tx(&tma_bar[buf], 128u * uint32_t(Gc) * uint32_t(R));
-        tc::tma_load_4d(sA + buf * 16384, t.map, 0, it.cg * Gc, 0, t.mz, &tma_bar[buf]);
-    };
-    // thread 0 only: bit b = parity of A tile b's next TMA completion
-    uint32_t tma_phases = 0;
     bool ok = true;
-    // thread 0: the item in A tile `buf` times B into accumulator `buf`
-    auto mma = [&](int buf) {
-        ok = tc::mbar_wait(&tma_bar[buf], (tma_phases >> buf) & 1u) && ok;
-        tma_phases ^= 1u << buf;
-        tc::fence_after();
-        const uint32_t a0 = tc::smem_u32(sA + buf * 16384), b0 = tc::smem_u32(sB);
-        constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kConvN);
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks)
-            tc::mma_u8(tbase + 64 * buf, tc::sw128_desc(a0 + 32 * ks), tc::sw128_desc(b0 + 32 * ks), idesc,
-                       ks > 0);
-        tc::mma_commit(&mma_bar[buf]);
-    };
-    if (tid == 0) {
-        if (begin < end) issue(begin, 0);
-        if (begin + 1 < end) issue(begin + 1, 1);
-    }
 
-    // column-stage role: prime j of the group, column c of the tile
-    const int cj = tid / 8, cc = tid % 8;
-    uint2 twr[R > 1 ? R - 1 : 1];
-    PrimeConst cpc{};
-    int cur_pg = -1;
-
-    uint32_t mma_phases = 0;  // bit b: parity of accumulator b's next MMA completion
-    int kk = 0;
-    for (int k = begin; k < end; ++k, ++kk) {
-        const ConvItem it = w.item(k);
-        const ConvTarget t = w.target(it.z, it.poly);
-        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
-        const int buf = kk & 1;
-        if (it.pg != cur_pg) {
-            // every MMA issued so far is complete and none reads B for this item yet: B may be rewritten
-            const uint4* src = reinterpret_cast<const uint4*>(conv_w + size_t(it.pg) * 8192);
-            for (int q = tid; q < 512; q += 128) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
-            if (tid < tc::kConvGroup) spc[tid] = pcs[it.pg * tc::kConvGroup + tid];
-            const int ci = it.pg * tc::kConvGroup + cj;
-#pragma unroll
-            for (int q = 1; q < R; ++q) twr[q - 1] = __ldg(tw_fwd + size_t(ci) * kNMax + q);
-            cpc = pcs[ci];
-            cur_pg = it.pg;
-            tc::fence_smem_async();
-            __syncthreads();
-            if (tid == 0) mma(buf);
+    if (warp == 4) {
+        // ------------------------------ producer ------------------------------
+        // every lane runs the loop (uniform control flow); lane 0 issues
+        auto issue = [&](int k, int buf) {
+            const ConvItem it = w.item(k);
+            const ConvTarget t = w.target(it.z, it.poly);
+            const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+            tc::mbar_expect_tx(&tma_full[buf], 128u * uint32_t(Gc) * uint32_t(R));
+            tc::tma_load_4d(sA + buf * 16384, t.map, 0, it.cg * Gc, 0, t.mz, &tma_full[buf]);
+        };
+        auto wait = [&](uint64_t* bar, uint32_t parity) {
+            const bool done = __all_sync(0xffffffffu, tc::mbar_wait(bar, parity));
+            ok = ok && done;
+            return done;
+        };
+        uint32_t ph_tma = 0, ph_mma = 0, ph_empty = 0, ph_b = 0, pending = 0;  // bit b: buffer b
+        bool b_pending = false;
+        if (lane == 0) {
+            if (begin < end) issue(begin, 0);
+            if (begin + 1 < end) issue(begin + 1, 1);
         }
-        const int np = min(tc::kConvGroup, t.P - it.pg * tc::kConvGroup);
-        ok = tc::mbar_wait(&mma_bar[buf], (mma_phases >> buf) & 1u) && ok;
-        mma_phases ^= 1u << buf;
-        tc::fence_after();
-        if (tid == 0) {
-            // this item's MMA has read A tile `buf`: load item k+2 into it
-            if (k + 2 < end) issue(k + 2, buf);
-            // the next item's MMA runs during this epilogue (its accumulator was
-            // drained before the previous item's closing barrier)
-            if (k + 1 < end && w.item(k + 1).pg == cur_pg) mma(buf ^ 1);
-        }
-        // --- residues of row m = tid for the group's 16 primes ---
-        // byte-plane sums d_a <= 128 * 255^2 < 2^23, so d0 + 2^8 d1 and d2 + 2^8 d3
-        // fit 32 bits and the residue input is (d2 + 2^8 d3) 2^16 + d0 + 2^8 d1 < 2^48
+        pending = (begin < end ? 1u : 0u) | (begin + 1 < end ? 2u : 0u);
+        int loaded_pg = -1, kk = 0;
+        for (int k = begin; k < end; ++k, ++kk) {
+            if (__any_sync(0xffffffffu, s_abort != 0)) break;  // a worker gave up a wait
+            const int buf = kk & 1;
+            const int pg = w.item(k).pg;
+            if (pg != loaded_pg) {  // every earlier MMA was waited for: B may be rewritten
+                if (lane == 0) {
+                    tc::mbar_expect_tx(&b_full, 8192u);
+                    tc::bulk_load(sB, conv_w + size_t(pg) * 8192, 8192u, &b_full);
+                }
+                b_pending = true;
+                if (!wait(&b_full, ph_b)) break;
+                ph_b ^= 1u;
+                b_pending = false;
+                loaded_pg = pg;
+            }
+            if (!wait(&tma_full[buf], (ph_tma >> buf) & 1u)) break;
+            ph_tma ^= 1u << buf;
+            pending &= ~(1u << buf);
+            if (kk >= 2) {
+                if (!wait(&tmem_empty[buf], (ph_empty >> buf) & 1u)) break;
+                ph_empty ^= 1u << buf;
+            }
+            tc::fence_after();
+            if (lane == 0) {
+                const uint32_t a0 = tc::smem_u32(sA + buf * 16384), b0 = tc::smem_u32(sB);
+                constexpr uint32_t idesc = tc::idesc_u8(tc::kTileM, tc::kConvN);
 #pragma unroll
-        for (int q4 = 0; q4 < 4; ++q4) {
-            uint32_t d[16];
-            tc::tmem_ld16(taddr + 64 * buf + 16 * q4, d);
-            tc::tmem_wait_ld();
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = 4 * q4 + u;
-                const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
-                const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
-                const uint64_t v = (uint64_t(hi) << 16) + lo;
-                sT[j * kTS + tid] = reduce60(v, spc[j].p, spc[j].mu);
+                for (int ks = 0; ks < 4; ++ks)
+                    tc::mma_u8(tbase + 64 * buf, tc::sw128_desc(a0 + 32 * ks), tc::sw128_desc(b0 + 32 * ks), idesc,
+                               ks > 0);
+                tc::mma_commit(&mma_full[buf]);
+            }
+            __syncwarp();
+            // the MMA has read its A tile (and B): the tile takes the item two ahead
+            if (!wait(&mma_full[buf], (ph_mma >> buf) & 1u)) break;
+            ph_mma ^= 1u << buf;
+            if (k + 2 < end) {
+                if (lane == 0) issue(k + 2, buf);
+                pending |= 1u << buf;
             }
         }
-        tc::fence_before();
-        __syncthreads();
-        // --- forward column stages in registers, then store ---
-        if (cj < np && cc < Gc) {
-            const int ci = it.pg * tc::kConvGroup + cj;
-            uint32_t v[R];
+        if (!ok) s_abort = 1;
+        // copies requested but not consumed land before the CTA's shared memory goes away
+        for (int b = 0; b < 2; ++b)
+            if (pending & (1u << b)) tc::mbar_wait(&tma_full[b], (ph_tma >> b) & 1u);
+        if (b_pending) tc::mbar_wait(&b_full, ph_b);
+    } else {
+        // ------------------------------ workers -------------------------------
+        const uint32_t taddr = tbase + (uint32_t(32 * warp) << 16);
+        // column-stage role: prime j of the group, column c of the tile
+        const int cj = tid / 8, cc = tid % 8;
+        uint2 twr[R > 1 ? R - 1 : 1];
+        PrimeConst cpc{};
+        int cur_pg = -1;
+        uint32_t ph_mma = 0;
+        int kk = 0;
+        for (int k = begin; k < end; ++k, ++kk) {
+            const ConvItem it = w.item(k);
+            const ConvTarget t = w.target(it.z, it.poly);
+            const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+            const int buf = kk & 1;
+            if (it.pg != cur_pg) {  // the previous item's closing barrier ended every read of spc
+                if (tid < tc::kConvGroup) spc[tid] = pcs[it.pg * tc::kConvGroup + tid];
+                const int ci = it.pg * tc::kConvGroup + cj;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = sT[cj * kTS + r * Gc + cc];
-#pragma unroll
-            for (int s = 0; s < LOGR; ++s) {
-                const int h = R >> (s + 1);
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (!(r & h)) ct_bfly(v[r], v[r + h], twr[(1 << s) + (r >> (LOGR - s)) - 1], cpc.p, cpc.two_p);
+                for (int q = 1; q < R; ++q) twr[q - 1] = __ldg(tw_fwd + size_t(ci) * kNMax + q);
+                cpc = pcs[ci];
+                cur_pg = it.pg;
+                tc::bar_sync(1, 128);
             }
-            uint32_t* dst = t.res + (size_t(it.poly) * t.P + ci) * t.n + size_t(it.cg) * Gc + cc;
+            const int np = min(tc::kConvGroup, t.P - it.pg * tc::kConvGroup);
+            ok = tc::mbar_wait(&mma_full[buf], (ph_mma >> buf) & 1u) && ok;
+            ph_mma ^= 1u << buf;
+            tc::fence_after();
+            // --- residues of row m = tid for the group's 16 primes ---
+            // byte-plane sums d_a <= 128 * 255^2 < 2^23, so d0 + 2^8 d1 and d2 + 2^8 d3
+            // fit 32 bits and the residue input is (d2 + 2^8 d3) 2^16 + d0 + 2^8 d1 < 2^48
 #pragma unroll
-            for (int r = 0; r < R; ++r) dst[size_t(r) << t.logC] = v[r];
+            for (int q4 = 0; q4 < 4; ++q4) {
+                uint32_t d[16];
+                tc::tmem_ld16(taddr + 64 * buf + 16 * q4, d);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int j = 4 * q4 + u;
+                    const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
+                    const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
+                    const uint64_t v = (uint64_t(hi) << 16) + lo;
+                    sT[j * kTS + tid] = reduce60(v, spc[j].p, spc[j].mu);
+                }
+            }
+            tc::fence_before();
+            tc::mbar_arrive(&tmem_empty[buf]);  // this thread's accumulator reads are complete
+            tc::bar_sync(1, 128);
+            // --- forward column stages in registers, then store ---
+            if (cj < np && cc < Gc) {
+                const int ci = it.pg * tc::kConvGroup + cj;
+                uint32_t v[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[r] = sT[cj * kTS + r * Gc + cc];
+#pragma unroll
+                for (int s = 0; s < LOGR; ++s) {
+                    const int h = R >> (s + 1);
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (!(r & h))
+                            ct_bfly(v[r], v[r + h], twr[(1 << s) + (r >> (LOGR - s)) - 1], cpc.p, cpc.two_p);
+                }
+                uint32_t* dst = t.res + (size_t(it.poly) * t.P + ci) * t.n + size_t(it.cg) * Gc + cc;
+#pragma unroll
+                for (int r = 0; r < R; ++r) dst[size_t(r) << t.logC] = v[r];
+            }
+            // sT is rewritten by the next item; a failed wait (or the producer's) ends the loop for all workers
+            if (tc::bar_sync_or(1, 128, !ok || s_abort)) break;
         }
-        __syncthreads();  // sT is rewritten by the next item
+        if (!ok) s_abort = 1;
     }
     tc::fence_before();
     __syncthreads();
@@ -310,7 +361,7 @@ __global__ void __launch_bounds__(128) k1t_convert(const __grid_constant__ Work 
         tc::fence_after();
         tc::tmem_dealloc(tbase, 128);
     }
-    if (!ok && tid == 0) atomicOr(err, 1u);
+    if (!ok) atomicOr(err, 1u);
 }
 
 // ---------------------------------------------------------------------------
