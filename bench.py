@@ -264,6 +264,47 @@ def device_inputs(torch, batch, n, limbs, q, seed):
     raise RuntimeError("rejection sampling did not converge")
 
 
+def run_plain(args, torch, plan, A, Bv, Cv, stream, batched_value):
+    """The plain single-product path on the same GPU: one product per call.
+
+    device: pm_multiply on device buffers, one launch sequence per product, CUDA-event timed;
+    host:   pm_multiply_host on pinned host buffers (the fherma_run call), wall-clock timed."""
+    K = min(64, A.shape[0])
+    sh = stream.cuda_stream
+
+    def dev_pass():
+        for k in range(K):
+            plan.multiply(A[k].data_ptr(), Bv[k].data_ptr(), Cv[k].data_ptr(), stream=sh)
+
+    for _ in range(max(args.warmup, 1)):
+        dev_pass()
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev_pass()
+    e1.record(stream)
+    e1.synchronize()
+    dev = K * args.steps / (e0.elapsed_time(e1) / 1000.0)
+
+    H = min(8, K)
+    ha = A[:H].cpu().pin_memory()
+    hb = Bv[:H].cpu().pin_memory()
+    hc = torch.empty_like(ha).pin_memory()
+    for k in range(H):
+        plan.multiply_host_ptr(ha[k].data_ptr(), hb[k].data_ptr(), hc[k].data_ptr())
+    t0 = time.perf_counter()
+    reps = max(args.steps // 2, 2)
+    for _ in range(reps):
+        for k in range(H):
+            plan.multiply_host_ptr(ha[k].data_ptr(), hb[k].data_ptr(), hc[k].data_ptr())
+    host = H * reps / (time.perf_counter() - t0)
+    return {"device_products_per_s": dev, "host_products_per_s": host,
+            "batched_over_plain_device": batched_value / dev,
+            "api": "pm_multiply (device buffers) and pm_multiply_host (pinned host buffers), one product per call",
+            "products": {"device": K * args.steps, "host": H * reps}}
+
+
 def run_uneven(args, torch, polymul):
     """64 products, N log-uniform over {1024..65536}, widths uniform in 200..868 bits
     (seed 4), as one autotuned graph; against the same products through per-product
@@ -528,6 +569,8 @@ def run_ours(args):
     total_products = B * args.steps * world
     value = total_products / (ms / 1000.0)
 
+    plain = run_plain(args, torch, plan, A, Bv, Cv, stream, value / world)
+
     # end to end through the C ABI host-buffer call, pinned host memory
     E = min(args.e2e_batch, B)
     ha = torch.empty((E, n, limbs), dtype=torch.int64, pin_memory=True)
@@ -644,6 +687,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "serving": serving,
             "batched_uneven": uneven,
+            "plain": plain,
             "clocks": clocks,
             "mismatches": mismatches,
         }

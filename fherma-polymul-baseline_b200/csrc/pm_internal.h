@@ -38,6 +38,7 @@ int profile_read(const char** names, uint64_t* launches, double* total_ms, uint3
 struct DeviceBasis {
     int device = 0;
     std::vector<uint32_t> primes;   // kPMax primes, descending
+    std::vector<uint32_t> inv1;     // [kPMax] psi^-brev(1): the inverse twiddle of the last column stage
     PrimeConst* d_pc = nullptr;     // [kPMax]
     uint2* d_tw_fwd = nullptr;      // [kPMax][kNMax] psi^brev(k)   (value, Shoup)
     uint2* d_tw_inv = nullptr;      // [kPMax][kNMax] psi^-brev(k)
@@ -87,7 +88,7 @@ struct PlanCore {
     DeviceBasis* basis = nullptr;
     uint32_t* d_mq = nullptr;      // [P][W] (P_total/p_i) mod q
     uint32_t* d_consts = nullptr;  // q[W], (-P_total mod q)[W]
-    uint2* d_scale = nullptr;      // [P] n^-1 (P_total/p_i)^-1 mod p_i
+    uint2* d_scale = nullptr;      // [2P] s_i = 2^32 n^-1 (P_total/p_i)^-1 mod p_i, then s_i psi_i^-brev(1)
     uint32_t* d_work = nullptr;    // [2][P][n] residue planes (plan-owned workspace)
     void* d_batch_work = nullptr;  // residue planes for a group of products (pm_multiply_batch)
     uint32_t batch_work_group = 0;

@@ -178,6 +178,7 @@ DeviceBasis& basis_for_device(int device) {
     const size_t P = B->primes.size();
     std::vector<PrimeConst> pc(P);
     std::vector<uint2> fwd(P * kNMax), inv(P * kNMax), pow(P * kPowWords);
+    B->inv1.assign(P, 0);
     auto fill = [&](size_t begin, size_t end) {
         std::vector<uint32_t> ppow(kNMax), ipow(kNMax);
         for (size_t i = begin; i < end; ++i) {
@@ -206,6 +207,7 @@ DeviceBasis& basis_for_device(int device) {
             for (int it = 0; it < 5; ++it) pinv *= 2u - p * pinv;
             pc[i].pinv = pinv;
             pc[i].recip = uint64_t(((unsigned __int128)1 << 64) / p);
+            B->inv1[i] = inv[i * kNMax + 1].x;
         }
     };
     unsigned nt = std::thread::hardware_concurrency();
@@ -309,7 +311,7 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     Words total{1};
     for (unsigned i = 0; i < P; ++i) total = multiply_small(total, basis->primes[i]);
     std::vector<uint32_t> mq(size_t(P) * W, 0), consts(2 * size_t(W), 0);
-    std::vector<uint2> scale(P);
+    std::vector<uint2> scale(2 * size_t(P));
     for (unsigned i = 0; i < P; ++i) {
         const uint32_t p = basis->primes[i];
         Words m = total;
@@ -321,6 +323,8 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
         const uint32_t r32 = uint32_t((uint64_t(1) << 32) % p);
         const uint32_t s = mulmod(mulmod(minv, ninv, p), r32, p);
         scale[i] = make_uint2(s, shoup_of(s, p));
+        const uint32_t sw = mulmod(s, basis->inv1[i], p);  // the tensor CRT folds s_i into its last stage
+        scale[P + i] = make_uint2(sw, shoup_of(sw, p));
     }
     const Words qpad = padded(q, W);
     Words pmod = mod(total, q);
@@ -555,7 +559,8 @@ void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uin
 void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c) {
     if (!s.d_io) {
         cuda_check(cudaMalloc(&s.d_io, 3 * s.io_bytes), "allocate plan I/O buffers");
-        cuda_check(cudaMallocHost(&s.h_stage, 3 * s.io_bytes), "allocate pinned staging");
+        // staging for a, b, c, then one word the device error flag is copied into
+        cuda_check(cudaMallocHost(&s.h_stage, 3 * s.io_bytes + 16), "allocate pinned staging");
     }
     auto pinned = [](const void* p) {
         cudaPointerAttributes at{};
@@ -586,8 +591,11 @@ void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* 
     void* dst = pc ? static_cast<void*>(c) : static_cast<void*>(stage + 2 * s.io_bytes);
     cuda_check(cudaMemcpyAsync(dst, dev + 2 * s.io_bytes, s.io_bytes, cudaMemcpyDeviceToHost, s.stream),
                "copy c to host");
+    // the error word rides on the same stream: no second round trip after the product
+    uint32_t* herr = reinterpret_cast<uint32_t*>(stage + 3 * s.io_bytes);
+    cuda_check(cudaMemcpyAsync(herr, s.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream), "read error word");
     cuda_check(cudaStreamSynchronize(s.stream), "product");
-    check_device_errors(s);
+    if (*herr) check_device_errors(s);
     if (!pc) std::memcpy(c, stage + 2 * s.io_bytes, s.io_bytes);
 }
 

@@ -124,6 +124,9 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
                 va[(m << KP) + l] = sa[idx];
                 vb[(m << KP) + l] = sb[idx];
             }
+        // the rows arrived unswizzled and the exchanges store swizzled: every thread
+        // has its values before any exchange store lands in this buffer
+        __syncthreads();
         row_transform<LOGC, KP>(va, vb, sa, sb, stf, sti, tid, pc);
         uint32_t* ga = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
 #pragma unroll

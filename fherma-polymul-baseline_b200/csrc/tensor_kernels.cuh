@@ -467,19 +467,31 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
             for (int r = 0; r < R; ++r) v[r] = sR[(r * t.P + i) * Gc + c];
             const uint2* tw = sTw + i * RT - 1;  // tw[k] = Psi_inv_rev[k], k >= 1
 #pragma unroll
-            for (int s = LOGR - 1; s >= 0; --s) {
+            for (int s = LOGR - 1; s >= 1; --s) {
                 const int h = R >> (s + 1);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
                     if (!(r & h)) gs_bfly(v[r], v[r + h], tw[(1 << s) + (r >> (LOGR - s))], pc.p, pc.two_p);
             }
+            // last stage (one twiddle per prime) with the CRT scale s_i folded in:
+            // x' = s_i (x + y), y' = s_i w (x - y); digits t_i in [0, 2p) (an extra p_i
+            // adds P to the CRT sum and 1 to its nearest quotient, which cancel)
             const uint2 sc = __ldg(t.scale + i);
+            if constexpr (LOGR > 0) {
+                const uint2 sw = __ldg(t.scale + t.P + i);
+#pragma unroll
+                for (int r = 0; r < R / 2; ++r) {
+                    const uint32_t x = v[r], y = v[r + R / 2];
+                    v[r] = shoup_mul(x + y, sc, pc.p);
+                    v[r + R / 2] = shoup_mul(x - y + pc.two_p, sw, pc.p);
+                }
+            } else {
+                v[0] = shoup_mul(v[0], sc, pc.p);
+            }
             const uint32_t ka = uint32_t(i) >> 5, kb = (4u * i) & 127u;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t x = csub(shoup_mul(v[r], sc, pc.p), pc.p);
-                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(r * Gc + c, kb)) = x;
-            }
+            for (int r = 0; r < R; ++r)
+                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(r * Gc + c, kb)) = v[r];
         }
         tc::fence_smem_async();
         tc::fence_before();

@@ -199,6 +199,10 @@ class Plan:
         check(lib().pm_multiply_host(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
         return c
 
+    def multiply_host_ptr(self, a_ptr, b_ptr, c_ptr):
+        """Same on raw host pointers (e.g. pinned torch tensors); synchronous."""
+        check(lib().pm_multiply_host(self._h, a_ptr, b_ptr, c_ptr))
+
     def autotune(self, reps=3):
         """Time candidate launch shapes and keep the fastest; returns them as a dict."""
         t = Tuning()
