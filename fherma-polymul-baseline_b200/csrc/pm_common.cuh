@@ -38,6 +38,13 @@ __device__ __forceinline__ uint32_t reduce60(uint64_t x, uint32_t p, uint32_t mu
     return csub(r, p);
 }
 
+// x mod p up to two extra p, for x < 2^60: the quotient estimate of reduce60
+// without its corrections, in [0, 3p) -- enough for a forward butterfly input.
+__device__ __forceinline__ uint32_t reduce60_lazy(uint64_t x, uint32_t p, uint32_t mu) {
+    const uint32_t q = uint32_t((uint64_t(uint32_t(x >> 29)) * mu) >> 32);
+    return uint32_t(x) - q * p;
+}
+
 // x * y * 2^-32 mod p up to one extra p, for x, y in [0, 2p): result in (0, 2p).
 // Montgomery reduction with m = lo(xy) p^-1: xy - m p is a multiple of 2^32 and,
 // as xy < 4p^2 < p 2^32, (xy - m p) / 2^32 lies in (-p, p).

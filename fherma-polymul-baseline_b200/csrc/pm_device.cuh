@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256) k1_convert_cols(const uint32_t* __restric
         uint64_t acc = 0;
 #pragma unroll
         for (int k = 0; k < W; ++k) acc += shoup_mul(x[k], cp[k], pc.p);
-        uint32_t v = reduce60(acc, pc.p, pc.mu);
+        uint32_t v = reduce60_lazy(acc, pc.p, pc.mu);  // [0, 3p): the column stages take [0, 4p)
         const uint2* tw = tw_fwd + size_t(i) * kNMax;
         for (int s = 0; s < logR; ++s) {
             const int bit = logR - 1 - s;
@@ -198,8 +198,7 @@ __device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, i
 #pragma unroll
             for (int l = 0; l < (1 << K); ++l) {
                 if (l & h) continue;
-                const uint2 w = tws[l >> (K - u)];
-                gs_bfly(v[(m << K) + l], v[(m << K) + l + h], w, p, two_p);
+                gs_bfly(v[(m << K) + l], v[(m << K) + l + h], tws[l >> (K - u)], p, two_p);
             }
         }
     }
@@ -291,7 +290,7 @@ __device__ __forceinline__ void k2_row_body(uint32_t* __restrict__ res, const Pr
     constexpr int C = 1 << LOGC;
     constexpr int T = C / 8;
     static_assert(KP == 2 || KP == 3, "pass radix");
-    extern __shared__ uint2 smem2[];
+    extern __shared__ __align__(16) uint2 smem2[];
     const int R = 1 << logR;
     uint2* stf = smem2 + sub * 2 * C;
     uint2* sti = stf + C;

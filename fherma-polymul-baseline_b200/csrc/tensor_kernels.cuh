@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
                     const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
                     const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
                     const uint64_t v = (uint64_t(hi) << 16) + lo;
-                    sT[j * kTS + tid] = reduce60(v, spc[j].p, spc[j].mu);
+                    sT[j * kTS + tid] = reduce60_lazy(v, spc[j].p, spc[j].mu);  // [0, 3p): butterfly input
                 }
             }
             tc::fence_before();
