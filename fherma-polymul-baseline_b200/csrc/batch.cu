@@ -249,6 +249,7 @@ struct BatchCore {
             d.P = int(p->P);
             d.W = int(p->W);
             d.sbits = int(p->qbits);
+            d.delta = p->delta;
             d.stride = int(p->stride);
             d.mu_q = p->mu_q;
             d.io_off = 2 * io_off[z];

@@ -441,16 +441,61 @@ __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_
     }
 }
 
+// v mod q for a special-form q = 2^k - delta (k = sbits >= 80, delta < 2^32;
+// the reference's FHERMA modulus 2^868 - 11993087 is one): with v = hi 2^k + lo,
+// v = lo + hi * delta (mod q), and lo + hi * delta < 2^k + 2^70 < 2q, so one
+// conditional subtraction finishes.  Same contract as reduce_mod_q otherwise.
+template <int W>
+__device__ __forceinline__ void reduce_special(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q, int k,
+                                               uint32_t delta) {
+    // hi = floor(v / 2^k) < 2^38 from words W-4 .. W+1; those words keep v mod 2^k
+    uint64_t hi = 0;
+#pragma unroll
+    for (int j = (W >= 4 ? W - 4 : 0); j < W + 2; ++j) {
+        const int pos = 32 * j - k;  // bit position of word j inside hi
+        if (pos > -32 && pos < 64) hi |= pos >= 0 ? uint64_t(v[j]) << pos : uint64_t(v[j]) >> (-pos);
+        if (32 * j >= k)
+            v[j] = 0;
+        else if (32 * j + 32 > k)
+            v[j] &= (1u << (k - 32 * j)) - 1u;
+    }
+    const uint64_t p0 = uint64_t(uint32_t(hi)) * delta, p1 = (hi >> 32) * delta;
+    const uint64_t mid = (p0 >> 32) + uint32_t(p1);
+    mp_add3<W + 2>(v, uint32_t(p0), uint32_t(mid), uint32_t(p1 >> 32) + uint32_t(mid >> 32));
+    uint32_t qq[W + 2], d[W + 2];
+#pragma unroll
+    for (int j = 0; j < W + 2; ++j) {
+        qq[j] = j < W ? q[j] : 0u;
+        d[j] = v[j];
+    }
+    const uint32_t borrowed = mp_sub<W + 2>(d, qq);
+#pragma unroll
+    for (int j = 0; j < W + 2; ++j) v[j] = borrowed ? v[j] : d[j];
+}
+
+// Reduction of the final CRT step: the general one, the special-form one, or
+// the one delta selects at run time (kernels whose products may be either).
+enum CrtReduction { kReduceGeneral = 0, kReduceSpecial = 1, kReduceEither = 2 };
+
 // Final CRT step shared by the SIMT and tensor paths: v += nearest *
 // (-P mod q), reduce mod q, store one coefficient (stride words).
-template <int W>
+template <int W, int RED = kReduceEither>
 __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t nearest, const uint32_t* s_q,
-                                           uint64_t mu_q, int sbits, uint32_t* dst, int stride) {
+                                           uint64_t mu_q, int sbits, uint32_t delta, uint32_t* dst, int stride) {
     uint32_t pneg[W];
 #pragma unroll
     for (int k = 0; k < W; ++k) pneg[k] = s_q[W + k];
     crt_mac<W>(v, nearest, pneg);
-    reduce_mod_q<W>(v, s_q, mu_q, sbits);
+    if constexpr (RED == kReduceSpecial) {
+        reduce_special<W>(v, s_q, sbits, delta);
+    } else if constexpr (RED == kReduceGeneral) {
+        reduce_mod_q<W>(v, s_q, mu_q, sbits);
+    } else {
+        if (delta)
+            reduce_special<W>(v, s_q, sbits, delta);
+        else
+            reduce_mod_q<W>(v, s_q, mu_q, sbits);
+    }
     if ((stride & 3) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
 #pragma unroll
         for (int k = 0; k < W; k += 4)
@@ -477,7 +522,8 @@ __global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ 
                                                    const uint2* __restrict__ tw_inv, const uint2* __restrict__ scale,
                                                    const uint32_t* __restrict__ mq,
                                                    const uint32_t* __restrict__ consts, uint64_t mu_q, int sbits,
-                                                   int n, int logR, int logC, int P, int stride, size_t io_bstride,
+                                                   uint32_t delta, int n, int logR, int logC, int P, int stride,
+                                                   size_t io_bstride,
                                                    size_t ws_bstride) {
     extern __shared__ uint32_t sm3[];
     __shared__ uint32_t s_q[2 * W];
@@ -531,7 +577,7 @@ __global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ 
     // nearest integer of sum t_i / p_i (the fraction is f1:f0 / 2^64)
     const uint32_t nearest = uint32_t((f1 + (1ull << 31)) >> 32);
     const size_t J = (size_t(r) << logC) + col0 + g;
-    crt_finish<W>(acc, nearest, s_q, mu_q, sbits, out + J * stride, stride);
+    crt_finish<W>(acc, nearest, s_q, mu_q, sbits, delta, out + J * stride, stride);
 }
 
 }  // namespace pm

@@ -85,6 +85,7 @@ struct PlanCore {
     uint32_t flags = 0;
     Words q;
     uint64_t mu_q = 0;
+    uint32_t delta = 0;      // q = 2^qbits - delta, delta < 2^32, PM_SPECIAL_FORM asked: folding reduction; else 0
     DeviceBasis* basis = nullptr;
     uint32_t* d_mq = nullptr;      // [P][W] (P_total/p_i) mod q
     uint32_t* d_consts = nullptr;  // q[W], (-P_total mod q)[W]

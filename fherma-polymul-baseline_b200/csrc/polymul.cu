@@ -276,7 +276,7 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     if (!q64 || q_limbs == 0) throw Failure(PM_ERR_INVALID, "q is missing");
     if (n_ < 2 || (n_ & (n_ - 1))) throw Failure(PM_ERR_INVALID, "n must be a power of two >= 2");
     if (n_ > uint32_t(kNMax)) throw Failure(PM_ERR_UNSUPPORTED, "n above 65536");
-    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR)) throw Failure(PM_ERR_INVALID, "unknown flags");
+    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_SPECIAL_FORM)) throw Failure(PM_ERR_INVALID, "unknown flags");
     q.assign(2 * q_limbs, 0);
     for (uint32_t i = 0; i < q_limbs; ++i) {
         q[2 * i] = uint32_t(q64[i]);
@@ -338,6 +338,14 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     divmod(num, q, &quo, nullptr);
     quo.resize(2, 0);
     mu_q = (uint64_t(quo[1]) << 32) | quo[0];
+    // special form q = 2^qbits - delta, delta < 2^32 (on request): the CRT folds 2^qbits = delta
+    delta = 0;
+    if (qbits >= 80 && (flags & PM_SPECIAL_FORM)) {
+        Words top(qbits / 32 + 1, 0);
+        top[qbits / 32] = 1u << (qbits % 32);
+        const Words d = subtract(top, q);
+        if (bit_length(d) <= 32) delta = d.empty() ? 0u : d[0];
+    }
 
     workspace_bytes = size_t(2) * P * n * sizeof(uint32_t);
     io_bytes = size_t(n) * coef_limbs * sizeof(uint64_t);
@@ -407,7 +415,8 @@ void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, const Batch
         cuda_check(cudaFuncSetAttribute(k3_cols_crt<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "raise K3 shared memory");
     k3_cols_crt<W><<<grid, block, smem, st>>>(work, c, s.basis->d_pc, s.basis->d_tw_inv, s.d_scale, s.d_mq,
-                                              s.d_consts, s.mu_q, int(s.qbits), int(s.n), int(s.logR), int(s.logC),
+                                              s.d_consts, s.mu_q, int(s.qbits), s.delta, int(s.n), int(s.logR),
+                                              int(s.logC),
                                               int(s.P), int(s.stride), bt.io_bstride, bt.ws_bstride);
 }
 

@@ -178,8 +178,9 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     int ctas = sm_count() * s.tune.crt_ctas_per_sm;
     if (ctas > items) ctas = items;
     const size_t smem = k3t_smem_bytes<LOGR>();
-    cuda_check(cudaFuncSetAttribute(k3t_crt<LOGR, W, PlanCrtWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(smem)),
+    // one plan, one q: the reduction is chosen here rather than per coefficient
+    auto kernel = s.delta ? k3t_crt<LOGR, W, PlanCrtWork, kReduceSpecial> : k3t_crt<LOGR, W, PlanCrtWork, kReduceGeneral>;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K3T shared memory");
     PlanCrtWork w;
     std::memset(&w.map_res, 0, sizeof w.map_res);
@@ -194,12 +195,13 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     w.crt_w = s.d_crt_weights;
     w.mu_q = s.mu_q;
     w.sbits = int(s.qbits);
+    w.delta = s.delta;
     w.n = int(s.n);
     w.logC = int(s.logC);
     w.P = int(s.P);
     w.stride = int(s.stride);
     w.count = int(count);
-    k3t_crt<LOGR, W, PlanCrtWork><<<ctas, 128, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_inv, s.d_err);
+    kernel<<<ctas, 128, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_inv, s.d_err);
 }
 
 template <int LOGR>

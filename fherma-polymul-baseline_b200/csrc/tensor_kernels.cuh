@@ -60,11 +60,13 @@ struct CrtTarget {
     const uint8_t* crt_w;    // [2][128][128] pre-swizzled CRT weights
     uint64_t mu_q;
     int sbits, n, logC, P, stride, use_tma;
+    uint32_t delta;          // special-form q = 2^sbits - delta, or 0
 };
 
 // Per-product descriptor of an uneven batch (device table).
 struct BatchProduct {
     int n, logC, P, W, sbits, stride;
+    uint32_t delta;  // special-form q = 2^sbits - delta, or 0
     uint64_t mu_q;
     uint64_t io_off;  // u32 words from the batch's a (b, c) base to this product
     uint64_t ws_off;  // u32 words from the batch's workspace base to its planes
@@ -119,12 +121,13 @@ struct PlanCrtWork {
     const uint8_t* crt_w;
     uint64_t mu_q;
     int sbits, n, logC, P, stride, count, use_tma;
+    uint32_t delta;
     __device__ int lg() const { return logC - min(logC, 3); }  // column groups per row = 2^lg
     __device__ int total() const { return count << lg(); }
     __device__ int2 item(int k) const { return make_int2(k >> lg(), k & ((1 << lg()) - 1)); }
     __device__ CrtTarget target(int z) const {
         return CrtTarget{&map_res, z, work + z * ws_bstride, out + z * io_bstride, scale, consts, crt_w, mu_q,
-                         sbits, n, logC, P, stride, use_tma};
+                         sbits, n, logC, P, stride, use_tma, delta};
     }
 };
 
@@ -143,7 +146,7 @@ struct TableCrtWork {
     __device__ CrtTarget target(int z) const {
         const BatchProduct& d = prod[z];
         return CrtTarget{maps + 3 * z + 2, 0, work + d.ws_off, out + d.io_off, d.scale, d.consts, d.crt_w,
-                         d.mu_q, d.sbits, d.n, d.logC, d.P, d.stride, 1};
+                         d.mu_q, d.sbits, d.n, d.logC, d.P, d.stride, 1, d.delta};
     }
 };
 
@@ -378,7 +381,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB,
 // residue box 64*R*8 words, inverse column twiddles 64*(R-1) uint2.
 // ---------------------------------------------------------------------------
-template <int LOGR, int W, class Work>
+template <int LOGR, int W, class Work, int RED = kReduceEither>
 __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs,
                                                const uint2* __restrict__ tw_inv, uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
@@ -545,7 +548,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         const int rr = tid / Gc, cc = tid % Gc;
         if (rr < R) {
             const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
-            crt_finish<W>(acc, nearest, s_q, t.mu_q, t.sbits, t.out + J * t.stride, t.stride);
+            crt_finish<W, RED>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride);
         }
         tc::fence_before();
         __syncthreads();

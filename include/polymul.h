@@ -42,7 +42,13 @@ enum pm_status {
 /* Residue conversion and CRT implementation. */
 enum pm_flags {
     PM_CONVERT_SIMT = 0,   /* scalar CUDA-core conversion and CRT (the plain method) */
-    PM_CONVERT_TENSOR = 1  /* exact INT8 digit contractions on the tcgen05 tensor cores */
+    PM_CONVERT_TENSOR = 1, /* exact INT8 digit contractions on the tcgen05 tensor cores */
+    /* For a q of the special form 2^k - delta (k >= 80, delta < 2^32, e.g. the FHERMA modulus
+     * 2^868 - 11993087; the family the reference's quartic backend targets,
+     * quartic/host_setup.h:41-110), reduce the CRT sum by folding 2^k = delta instead of by the
+     * general Barrett division.  Same results; ignored for other q.  Measured no faster on
+     * B200 (the CRT kernel is bound by latency, not by this step), so it is not the default. */
+    PM_SPECIAL_FORM = 2
 };
 
 typedef struct {
