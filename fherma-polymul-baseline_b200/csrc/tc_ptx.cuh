@@ -24,8 +24,8 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-// Bounded wait on an mbarrier phase; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase; false when it gave up (after limit_ns).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
     const uint64_t start = global_ns();
     while (true) {
         uint32_t done;
@@ -37,7 +37,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (done) return true;
-        if (global_ns() - start > kWaitNs) return false;
+        if (global_ns() - start > limit_ns) return false;
     }
 }
 

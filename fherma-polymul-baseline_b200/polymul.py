@@ -148,6 +148,15 @@ def profile_read():
     return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(min(cap, count.value))}
 
 
+def selftest_bounded_wait(limit_us):
+    """Run the library's bounded device wait on a barrier nothing arrives at; returns
+    (timed_out, waited_ns)."""
+    t = ctypes.c_uint32(0)
+    w = ctypes.c_uint64(0)
+    check(lib().pm_selftest_bounded_wait(ctypes.c_uint32(limit_us), ctypes.byref(t), ctypes.byref(w)))
+    return bool(t.value), w.value
+
+
 class Plan:
     """A product plan for (n, q): basis, CRT constants, workspace, staging."""
 

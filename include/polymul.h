@@ -242,6 +242,15 @@ const char* pm_last_error(void);
 uint64_t pm_kernel_launch_count(void);
 
 /*
+ * Diagnostic (no counterpart in the reference): runs the library's bounded
+ * mbarrier wait on a barrier that nothing arrives at, with a limit of limit_us
+ * (1 .. 2e6) instead of the kernels' 1 s.  *timed_out = 1 when the wait gave up,
+ * *waited_ns = how long it waited.  Shows that a device wait that cannot finish
+ * ends with an error status and leaves the CUDA context usable.
+ */
+int pm_selftest_bounded_wait(uint32_t limit_us, uint32_t* timed_out, uint64_t* waited_ns);
+
+/*
  * Kernel timing for measurement runs.  pm_profile_enable(capacity) makes the
  * library record a CUDA event before and after each kernel it launches, on the
  * launching stream, for up to `capacity` launches (0 switches it off and drops

@@ -42,6 +42,10 @@ def test_invalid_arguments_fail_before_cuda():
     assert e.value.status == polymul.PM_ERR_UNSUPPORTED
     with pytest.raises(polymul.PolymulError):
         polymul.Plan(32, (1 << 868) - 11993087, coef_limbs=13)
+    for limit in (0, 2_000_001):
+        with pytest.raises(polymul.PolymulError) as e:
+            polymul.selftest_bounded_wait(limit)
+        assert e.value.status == polymul.PM_ERR_INVALID
 
 
 def test_status_strings():
