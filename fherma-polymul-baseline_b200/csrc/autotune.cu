@@ -8,8 +8,8 @@
 //   crt_ctas_per_sm  persistent CTAs of the tensor CRT per SM;
 //   row_persistent   K2 as one CTA per row, or as the persistent kernel that
 //                    stages each row's twiddles once per group and prefetches;
-//   group            products per launch group in batched calls (larger groups
-//                    fill the GPU, smaller ones keep residue planes in L2).
+//   group            products per launch group in batched calls, 4..64 (larger
+//                    groups amortize each persistent kernel's set-up and tail).
 // Coordinate descent from the defaults, objective = device time per product of
 // a batched call; results are cached per (n, bits(q), coef_limbs, path) for the
 // life of the process, so later plans with the same shape reuse them.
@@ -59,10 +59,10 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
         }
     }
     if (reps == 0) reps = 3;
-    // a batch big enough to fill the GPU, capped at ~1.5 GB of buffers
+    // a batch big enough for the largest group tried, capped at ~2 GB of buffers
     const size_t per = 3 * s.io_bytes + s.workspace_bytes;
-    uint32_t count = uint32_t((size_t(1536) << 20) / per);
-    count = count < 1 ? 1 : (count > 16 ? 16 : count);
+    uint32_t count = uint32_t((size_t(2048) << 20) / per);
+    count = count < 1 ? 1 : (count > 64 ? 64 : count);
     Scratch sc;
     cuda_check(cudaStreamCreateWithFlags(&sc.st, cudaStreamNonBlocking), "autotune stream");
     cuda_check(cudaEventCreate(&sc.e0), "autotune event");
@@ -125,7 +125,7 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
             if (k != best.crt_ctas_per_sm) consider(t);
         }
     }
-    for (uint32_t g : {1u, 2u, 4u, 8u, 16u}) {
+    for (uint32_t g : {4u, 8u, 16u, 32u, 64u}) {
         if (g > count) break;
         Tuning t = best;
         t.group = g;

@@ -69,7 +69,7 @@ struct Tuning {
     int conv_ctas_per_sm = 4;  // K1T persistent CTAs per SM (per prime group share)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
     bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)
-    uint32_t group = 0;        // products per launch group in batches (0: fit ~64 MB of residues)
+    uint32_t group = 0;        // products per launch group in batches (0: up to ~1 GB of residues, <= 64)
     bool tuned = false;
 };
 

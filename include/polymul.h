@@ -78,7 +78,7 @@ typedef struct {
     uint32_t row_radix;         /* radix of the row NTT register passes: 4 or 8 */
     uint32_t conv_ctas_per_sm;  /* persistent CTAs of the tensor conversion per SM, 1..8 */
     uint32_t crt_ctas_per_sm;   /* persistent CTAs of the tensor CRT per SM, 1..4 */
-    uint32_t group;             /* products per launch group in batched calls (0: fit ~64 MB of residues) */
+    uint32_t group;             /* products per launch group in batched calls (0: up to ~1 GB of residues, <= 64) */
     uint32_t row_persistent;    /* 1: rows of >= 1024 values by the persistent kernel that stages a row's
                                    twiddles once per group and prefetches rows; 0: one CTA per row */
     double us_per_product;      /* device time the autotuner measured (-1: taken from its cache) */
