@@ -299,9 +299,26 @@ def run_plain(args, torch, plan, A, Bv, Cv, stream, batched_value):
         for k in range(H):
             plan.multiply_host_ptr(ha[k].data_ptr(), hb[k].data_ptr(), hc[k].data_ptr())
     host = H * reps / (time.perf_counter() - t0)
+
+    # the plain method too: the same single-product calls with the SIMT conversion and CRT
+    import polymul
+    simt = polymul.Plan(plan.n, plan.q, coef_limbs=plan.coef_limbs, tensor=False)
+    for k in range(min(8, K)):
+        simt.multiply(A[k].data_ptr(), Bv[k].data_ptr(), Cv[k].data_ptr(), stream=sh)
+    stream.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        for k in range(K):
+            simt.multiply(A[k].data_ptr(), Bv[k].data_ptr(), Cv[k].data_ptr(), stream=sh)
+    e1.record(stream)
+    e1.synchronize()
+    simt_dev = K * args.steps / (e0.elapsed_time(e1) / 1000.0)
+    simt.close()
     return {"device_products_per_s": dev, "host_products_per_s": host,
+            "simt_method_device_products_per_s": simt_dev,
             "batched_over_plain_device": batched_value / dev,
-            "api": "pm_multiply (device buffers) and pm_multiply_host (pinned host buffers), one product per call",
+            "api": "pm_multiply (device buffers) and pm_multiply_host (pinned host buffers), one product per call; "
+                   "simt_method: PM_CONVERT_SIMT plan, pm_multiply per product",
             "products": {"device": K * args.steps, "host": H * reps}}
 
 
@@ -434,17 +451,17 @@ def run_serving(args, torch, polymul):
         pools[n] = (a, b, c)
     last_input = {}  # (n, ring slot) -> input index of the last request written there
 
-    def run(submit, drain):
+    def run(submit, drain, arr=arrivals, count_to=R):
         count = {n: 0 for n in SERVE_SIZES}
         t0 = time.perf_counter()
-        for k in range(R):
+        for k in range(count_to):
             n = int(sizes[k])
             j, r = count[n] % pool_k, count[n] % ring
             count[n] += 1
-            while time.perf_counter() - t0 < arrivals[k]:
+            while time.perf_counter() - t0 < arr[k]:
                 pass
             a, b, c = pools[n]
-            submit(n, a[j].data_ptr(), b[j].data_ptr(), c[r].data_ptr(), t0 + arrivals[k])
+            submit(n, a[j].data_ptr(), b[j].data_ptr(), c[r].data_ptr(), t0 + arr[k])
             last_input[(n, r)] = j
         drain()
         return time.perf_counter() - t0
@@ -457,6 +474,12 @@ def run_serving(args, torch, polymul):
     srv.reset_stats()
     wall = run(lambda n, pa, pb, pc, due: srv.submit_ptr(n, q, limbs, pa, pb, pc), srv.drain)
     st = srv.stats()
+    # saturation: the same mix queued all at once, what the loop sustains when the link is the limit
+    srv.reset_stats()
+    S = min(R, 4000)
+    sat_wall = run(lambda n, pa, pb, pc, due: srv.submit_ptr(n, q, limbs, pa, pb, pc), srv.drain,
+                   np.zeros(S), S)
+    sat = srv.stats()
     srv.close()
     mismatches = 0
     plans = {n: polymul.Plan(n, q, limbs) for n in SERVE_SIZES}
@@ -485,6 +508,9 @@ def run_serving(args, torch, polymul):
         "products_per_s": st["products_per_s"], "p50_us": st["p50_us"], "p99_us": st["p99_us"],
         "mean_us": st["mean_us"], "wall_s": wall, "groups": st["groups"], "peak_inflight": st["peak_inflight"],
         "peak_group": st["peak_group"], "mismatches": mismatches,
+        "saturated": {"requests": S, "products_per_s": S / sat_wall, "p50_us": sat["p50_us"], "p99_us": sat["p99_us"],
+                      "peak_inflight": sat["peak_inflight"], "peak_group": sat["peak_group"],
+                      "note": "all requests queued at t=0: latency is queueing time"},
         "plain_in_turn": {"products_per_s": R / plain_wall, "p50_us": pct(lat, 0.5), "p99_us": pct(lat, 0.99),
                           "api": "pm_multiply_host, one request at a time"},
     }
