@@ -65,6 +65,7 @@ extern "C" int pm_multiply_noalloc(const pm_plan* plan, const uint64_t* a, const
         int device = -1;
         pm::cuda_check(cudaGetDevice(&device), "cudaGetDevice");
         if (device != s.device) return pm::fail(PM_ERR_INVALID, "the plan belongs to another device");
+        pm::check_device_pointers(s, a, b, c, nullptr);
         pm::launch_product(s, a, b, c, pm::scratch_address(device), reinterpret_cast<cudaStream_t>(stream));
         return PM_OK;
     } catch (const pm::Failure& f) {

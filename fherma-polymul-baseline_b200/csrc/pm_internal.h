@@ -121,6 +121,11 @@ void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32
 uint32_t group_size(const PlanCore& s);
 void launch_rows(const PlanCore& s, uint32_t* work, uint32_t count, cudaStream_t st);
 void check_device_errors(const PlanCore& s);
+// Device-pointer arguments a kernel may touch: reachable from the device (not
+// pageable host memory), 8-byte aligned (u64 coefficients; the kernels move 8
+// and 16 bytes at a time), and 16-byte aligned on the tensor path (tensor maps
+// of a, b and the residue workspace).  Throws PM_ERR_INVALID otherwise.
+void check_device_pointers(const PlanCore& s, const void* a, const void* b, const void* c, const void* workspace);
 void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
                   uint32_t group, void* workspace, cudaStream_t st);
 void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,

@@ -520,6 +520,27 @@ void launch_simt(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32
     count_launches(3);
 }
 
+void check_device_pointers(const PlanCore& s, const void* a, const void* b, const void* c, const void* workspace) {
+    const void* ptrs[4] = {a, b, c, workspace};
+    const char* names[4] = {"a", "b", "c", "workspace"};
+    for (int i = 0; i < 4; ++i) {
+        if (!ptrs[i]) continue;
+        const uintptr_t addr = reinterpret_cast<uintptr_t>(ptrs[i]);
+        const uintptr_t need = (s.flags & PM_CONVERT_TENSOR) && i != 2 ? 16 : 8;
+        if (addr % need)
+            throw Failure(PM_ERR_INVALID, std::string(names[i]) + " must be " + std::to_string(need) +
+                                              "-byte aligned");
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, ptrs[i]) != cudaSuccess) {
+            cudaGetLastError();
+            throw Failure(PM_ERR_INVALID, std::string(names[i]) + " is not a pointer the device can use");
+        }
+        if (at.type == cudaMemoryTypeUnregistered)
+            throw Failure(PM_ERR_INVALID, std::string(names[i]) +
+                                              " is pageable host memory: pass device, managed or pinned memory");
+    }
+}
+
 // A kernel that gave up a bounded wait records it in the plan's error word.
 void check_device_errors(const PlanCore& s) {
     if (!s.d_err) return;
@@ -769,7 +790,10 @@ extern "C" int pm_plan_destroy(pm_plan* plan) {
 extern "C" int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                            pm_stream stream) {
     if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
-    PM_GUARD(pm::launch_product(plan->core, a, b, c, workspace, reinterpret_cast<cudaStream_t>(stream)))
+    PM_GUARD({
+        pm::check_device_pointers(plan->core, a, b, c, workspace);
+        pm::launch_product(plan->core, a, b, c, workspace, reinterpret_cast<cudaStream_t>(stream));
+    })
 }
 
 extern "C" int pm_batch_workspace_size(const pm_plan* plan, uint32_t count, size_t* bytes) {
@@ -785,6 +809,7 @@ extern "C" int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_
     if (count == 0) return PM_OK;
     PM_GUARD({
         auto& s = plan->core;
+        pm::check_device_pointers(s, a, b, c, workspace);
         uint32_t g = pm::group_size(s);
         if (g > count) g = count;
         if (workspace) {

@@ -103,6 +103,10 @@ int pm_plan_destroy(pm_plan* plan);
  * device buffer of info.workspace_bytes, or NULL to use the plan's own (then
  * calls on one plan must not overlap).  Replaces the device half of fherma_run
  * (rns/solve.cu:504-578, launch_rns).
+ * Pointers must be device, managed or pinned memory, 8-byte aligned; on the
+ * tensor path a, b and workspace 16-byte aligned (cudaMalloc gives 256):
+ * otherwise PM_ERR_INVALID, before anything runs.  The same holds for
+ * pm_multiply_batch and pm_multiply_noalloc.
  */
 int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                 pm_stream stream);

@@ -233,3 +233,35 @@ def test_tunings_do_not_change_results(cuda, path, n):
     for k in (0, count - 1):
         ak, bk = a[k].cpu().numpy().view(np.uint64), b[k].cpu().numpy().view(np.uint64)
         assert (ref[k].cpu().numpy().view(np.uint64) == oracle.rns_multiply(ak, bk, q)).all()
+
+
+def test_bad_device_pointers_are_refused(cuda, path):
+    """Misaligned or pageable pointers are caught on the host, before any kernel runs."""
+    torch = cuda
+    n, limbs = 1024, limbs_for(path, 868)
+    rng = np.random.default_rng(8)
+    q = random_q(rng, 868)
+    a = torch.from_numpy(uniform_below(rng, q, n, limbs).view(np.int64)).cuda()
+    b = torch.from_numpy(uniform_below(rng, q, n, limbs).view(np.int64)).cuda()
+    c = torch.zeros_like(a)
+    raw = torch.zeros(a.numel() * 8 + 64, dtype=torch.uint8, device="cuda")
+    host = np.zeros((n, limbs), dtype=np.uint64)  # pageable
+    with make_plan(path, n, q, limbs) as p:
+        for args in [(a.data_ptr() + 4, b.data_ptr(), c.data_ptr()),
+                     (a.data_ptr(), b.data_ptr(), c.data_ptr() + 4),
+                     (a.data_ptr(), host.ctypes.data, c.data_ptr())]:
+            with pytest.raises(polymul.PolymulError) as e:
+                p.multiply(*args)
+            assert e.value.status == polymul.PM_ERR_INVALID
+        if path == "tensor":
+            with pytest.raises(polymul.PolymulError) as e:
+                p.multiply(raw.data_ptr() + 8, b.data_ptr(), c.data_ptr())
+            assert e.value.status == polymul.PM_ERR_INVALID
+            with pytest.raises(polymul.PolymulError) as e:
+                p.multiply(a.data_ptr(), b.data_ptr(), c.data_ptr(), workspace=raw.data_ptr() + 8)
+            assert e.value.status == polymul.PM_ERR_INVALID
+        # the plan still works afterwards
+        p.multiply(a.data_ptr(), b.data_ptr(), c.data_ptr())
+        torch.cuda.synchronize()
+        got = c.cpu().numpy().view(np.uint64)
+        assert (got == oracle.rns_multiply(a.cpu().numpy().view(np.uint64), b.cpu().numpy().view(np.uint64), q)).all()
