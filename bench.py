@@ -517,8 +517,9 @@ def run_serving(args, torch, polymul):
 
 
 def algorithmic_bytes(n, primes, limbs):
-    """Mandatory HBM bytes of each kernel per product (SURVEY-style count: inputs
-    read once, residue planes written/read once, output written once)."""
+    """Mandatory HBM bytes of each kernel per product: inputs read once, residue
+    planes written and read once, output written once (twiddle and table reads are
+    implementation overhead and not counted)."""
     io = n * 8 * limbs
     conv = 2 * io + 2 * primes * n * 4
     rows = 2 * primes * n * 4 + primes * n * 4
@@ -720,6 +721,26 @@ def run_ours(args):
                     "algorithmic_bytes_per_launch": per_launch,
                     "algorithmic_bytes_per_product": alg[dom]}
 
+    # INT8 tensor-core contractions (tensor path): algorithmic INT8 ops per product over each
+    # kernel's device time, against the INT8 dense peak taken as twice the measured bf16 GEMM rate
+    # (B200: 4.5 vs 2.25 PFLOP/s nominal); the MMAs issue more (K padded to 128 and 256 bytes)
+    tensor_pipe = None
+    if args.path == "tensor":
+        digits = (bits + 7) // 8
+        ops = {"k1t_convert_cols": 2 * (2 * n) * digits * 4 * plan.primes,
+               "k3t_cols_crt": 2 * n * 4 * plan.primes * (digits + 3)}
+        bf16 = 1590.0
+        if os.path.exists(peaks_path):
+            bf16 = float(json.load(open(peaks_path)).get("bf16_tflops", bf16))
+        tensor_pipe = {}
+        for name, per in ops.items():
+            if name in prof:
+                cnt, tot = prof[name]
+                tops = per * timed_products / (tot / 1000.0) / 1e12
+                tensor_pipe[name] = {"int8_ops_per_product": per, "achieved_tops": tops,
+                                     "peak_tops": 2 * bf16, "frac": tops / (2 * bf16),
+                                     "peak_source": "2 x measured bf16" if os.path.exists(peaks_path) else "fallback"}
+
     serving = None
     if world == 1 and args.serve_requests > 0:
         serving = run_serving(args, torch, polymul)
@@ -774,6 +795,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "roofline": roofline,
             "alu_roofline": alu,
+            "tensor_pipe": tensor_pipe,
             "kernels": kernels,
             "cpu_baseline": cpu,
             "serving": serving,
