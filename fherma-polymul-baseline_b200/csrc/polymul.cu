@@ -689,9 +689,28 @@ void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
     const uint8_t* A = reinterpret_cast<const uint8_t*>(a);
     const uint8_t* B = reinterpret_cast<const uint8_t*>(b);
     uint8_t* Cc = reinterpret_cast<uint8_t*>(c);
-    uint32_t k = 0;
-    for (uint32_t z = 0; z < count; z += g, ++k) {
-        const uint32_t cnt = count - z < g ? count - z : g;
+    // chunk sizes ramp 1, 2, .. up to g and back down at the end: the first H2D and the
+    // last D2H, which nothing overlaps, move one product instead of g
+    std::vector<uint32_t> chunks, tail;
+    {
+        uint32_t left = count;
+        for (uint32_t sz = 1; sz < g && left > 2 * g; sz *= 2) {
+            chunks.push_back(sz);
+            left -= sz;
+        }
+        for (uint32_t sz = 1; sz < g && left > g + sz; sz *= 2) {
+            tail.push_back(sz);
+            left -= sz;
+        }
+        while (left) {
+            const uint32_t sz = left < g ? left : g;
+            chunks.push_back(sz);
+            left -= sz;
+        }
+        chunks.insert(chunks.end(), tail.rbegin(), tail.rend());
+    }
+    uint32_t k = 0, z = 0;
+    for (const uint32_t cnt : chunks) {
         PipelineSlot& sl = *s.pipe[k % 3];
         const size_t bytes = size_t(cnt) * io;
         if (sl.pending) {  // the slot's previous chunk must be out before its buffers are reused
@@ -724,6 +743,8 @@ void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
         cuda_check(cudaEventRecord(sl.done, sl.stream), "pipeline event");
         outs[k % 3] = Out{out, pc ? nullptr : land, bytes};
         sl.pending = true;
+        z += cnt;
+        ++k;
     }
     for (int i = 0; i < 3; ++i) {
         PipelineSlot& sl = *s.pipe[i];
