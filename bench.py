@@ -323,9 +323,10 @@ def run_plain(args, torch, plan, A, Bv, Cv, stream, batched_value):
 
 
 def run_special(args, torch, polymul, tuning):
-    """The reference's FHERMA modulus q = 2^868 - 11993087, a special-form q: device products/s
+    """The reference's FHERMA modulus q = 2^868 - 11993087, a special-form prime: device products/s
     with the folding reduction (PM_SPECIAL_FORM) and with the general one (the default), same
-    batch and launch shapes, bit-identical results checked."""
+    batch and launch shapes, bit-identical results checked; and through the direct wide-modulus
+    NTT (PM_WIDE_NTT), the reference's wide backend, for comparison."""
     import numpy as np
 
     n, limbs = args.ring, 14
@@ -358,6 +359,23 @@ def run_special(args, torch, polymul, tuning):
         plan.close()
     out["identical"] = bool(all((results[0] == results[1]).flatten()))
     out["speedup"] = out["special_form_products_per_s"] / out["general_reduction_products_per_s"]
+    # the direct wide-modulus NTT (PM_WIDE_NTT) on the same prime, for comparison: 64 products
+    Bw = min(B, 64)
+    wide = polymul.Plan(n, q, coef_limbs=limbs, wide=True)
+    Cw = torch.empty_like(A[:Bw])
+    st = torch.cuda.Stream()
+    wide.multiply_batch(A.data_ptr(), Bv.data_ptr(), Cw.data_ptr(), Bw, stream=st.cuda_stream)
+    st.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(max(args.steps // 2, 1)):
+        wide.multiply_batch(A.data_ptr(), Bv.data_ptr(), Cw.data_ptr(), Bw, stream=st.cuda_stream)
+    e1.record(st)
+    e1.synchronize()
+    out["wide_ntt_products_per_s"] = Bw * max(args.steps // 2, 1) / (e0.elapsed_time(e1) / 1000.0)
+    out["wide_ntt_identical"] = bool((Cw[:4].cpu().numpy().view(np.uint64) == results[1]).all())
+    out["rns_over_wide"] = out["general_reduction_products_per_s"] / out["wide_ntt_products_per_s"]
+    wide.close()
     del A, Bv
     torch.cuda.empty_cache()
     return out

@@ -5,6 +5,8 @@ specialization per width W (python gen_crt_mac.py > crt_mac.cuh):
   mp_sub<N>(a[N], b[N]) -> mask     a -= b, mask = 0xffffffff if it borrowed out, else 0
   mp_sub_hi<W>(a[W+2], b[W+2])      a -= b * 2^32 (b[W+1] must be 0)
   mp_add3<N>(a[N], t0, t1, t2)      a += t2 * 2^64 + t1 * 2^32 + t0 (carry out of a[N-1] dropped)
+  mp_add<N>(a[N], b[N]) -> carry    a += b, carry = 1 if it carried out, else 0
+(mp_sub and mp_add for N = W and N = W + 2.)
 """
 WIDTHS = [4, 8, 12, 16, 20, 24, 28]
 
@@ -40,6 +42,15 @@ def sub_hi_body(W):
     return "\\n\\t".join(lines)
 
 
+def add_body(N):
+    a = [f"%{i + 1}" for i in range(N)]
+    b = [f"%{N + 1 + i}" for i in range(N)]
+    lines = [f"add.cc.u32 {a[0]}, {a[0]}, {b[0]};"]
+    lines += [f"addc.cc.u32 {a[k]}, {a[k]}, {b[k]};" for k in range(1, N)]
+    lines += ["addc.u32 %0, 0, 0;"]
+    return "\\n\\t".join(lines)
+
+
 def add3_body(N):
     a = [f"%{i}" for i in range(N)]
     lines = [f"add.cc.u32 {a[0]}, {a[0]}, %{N};", f"addc.cc.u32 {a[1]}, {a[1]}, %{N + 1};",
@@ -56,7 +67,8 @@ def main():
            "template <int W> __device__ __forceinline__ void crt_mac(uint32_t (&a)[W + 2], uint32_t t, const uint32_t (&m)[W]);",
            "template <int N> __device__ __forceinline__ uint32_t mp_sub(uint32_t (&a)[N], const uint32_t (&b)[N]);",
            "template <int W> __device__ __forceinline__ void mp_sub_hi(uint32_t (&a)[W + 2], const uint32_t (&b)[W + 2]);",
-           "template <int N> __device__ __forceinline__ void mp_add3(uint32_t (&a)[N], uint32_t t0, uint32_t t1, uint32_t t2);"]
+           "template <int N> __device__ __forceinline__ void mp_add3(uint32_t (&a)[N], uint32_t t0, uint32_t t1, uint32_t t2);",
+           "template <int N> __device__ __forceinline__ uint32_t mp_add(uint32_t (&a)[N], const uint32_t (&b)[N]);"]
     for W in WIDTHS:
         outs = ", ".join(f'"+r"(a[{i}])' for i in range(W + 2))
         ins = ", ".join(f'"r"(m[{i}])' for i in range(W)) + ', "r"(t)'
@@ -64,15 +76,23 @@ def main():
                    f"const uint32_t (&m)[{W}]) {{")
         out.append(f'    asm("{mac_body(W)}"\n        : {outs}\n        : {ins});')
         out.append("}")
+        for N in (W, W + 2):
+            outs = '"=r"(mask), ' + ", ".join(f'"+r"(a[{i}])' for i in range(N))
+            ins = ", ".join(f'"r"(b[{i}])' for i in range(N))
+            out.append(f"template <> __device__ __forceinline__ uint32_t mp_sub<{N}>(uint32_t (&a)[{N}], "
+                       f"const uint32_t (&b)[{N}]) {{")
+            out.append("    uint32_t mask;")
+            out.append(f'    asm("{sub_body(N)}"\n        : {outs}\n        : {ins});')
+            out.append("    return mask;")
+            out.append("}")
+            outs = '"=r"(carry), ' + ", ".join(f'"+r"(a[{i}])' for i in range(N))
+            out.append(f"template <> __device__ __forceinline__ uint32_t mp_add<{N}>(uint32_t (&a)[{N}], "
+                       f"const uint32_t (&b)[{N}]) {{")
+            out.append("    uint32_t carry;")
+            out.append(f'    asm("{add_body(N)}"\n        : {outs}\n        : {ins});')
+            out.append("    return carry;")
+            out.append("}")
         N = W + 2
-        outs = '"=r"(mask), ' + ", ".join(f'"+r"(a[{i}])' for i in range(N))
-        ins = ", ".join(f'"r"(b[{i}])' for i in range(N))
-        out.append(f"template <> __device__ __forceinline__ uint32_t mp_sub<{N}>(uint32_t (&a)[{N}], "
-                   f"const uint32_t (&b)[{N}]) {{")
-        out.append("    uint32_t mask;")
-        out.append(f'    asm("{sub_body(N)}"\n        : {outs}\n        : {ins});')
-        out.append("    return mask;")
-        out.append("}")
         outs = ", ".join(f'"+r"(a[{i}])' for i in range(N))
         ins = ", ".join(f'"r"(b[{i}])' for i in range(N - 1))
         out.append(f"template <> __device__ __forceinline__ void mp_sub_hi<{W}>(uint32_t (&a)[{N}], "

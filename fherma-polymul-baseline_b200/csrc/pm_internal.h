@@ -73,6 +73,17 @@ struct Tuning {
     bool tuned = false;
 };
 
+// Tables of the direct wide-modulus NTT (PM_WIDE_NTT, wide.cu).
+struct WideTables {
+    uint32_t* d_q = nullptr;      // [W]
+    uint32_t* d_r2 = nullptr;     // [W] R^2 mod q, R = 2^(32W)
+    uint32_t* d_ninv = nullptr;   // [W] n^-1 mod q
+    uint32_t* d_tw_fwd = nullptr; // [n][W] psi^brev(k) R mod q
+    uint32_t* d_tw_inv = nullptr; // [n][W] psi^-brev(k) R mod q
+    uint32_t qinv = 0;            // -q^-1 mod 2^32
+    ~WideTables();
+};
+
 // Everything one (n, q) product needs on the device.
 struct PlanCore {
     int device = 0;
@@ -103,6 +114,8 @@ struct PlanCore {
     uint32_t* d_err = nullptr;     // set by a kernel whose bounded wait ran out
     uint32_t tensor_k_crt = 0;
 
+    std::unique_ptr<WideTables> wide;  // set for PM_WIDE_NTT plans
+
     Tuning tune;
     std::unique_ptr<PipelineSlot> pipe[3];
     uint32_t pipe_group = 0;
@@ -132,6 +145,12 @@ void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uin
                     cudaStream_t st);
 void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c);
 void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count);
+
+// direct wide-modulus NTT (wide.cu)
+void wide_init(PlanCore& s);
+size_t wide_workspace_bytes(const PlanCore& s);
+void launch_wide(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
+                 uint32_t count, cudaStream_t st);
 
 // tensor-core conversion / CRT (tensor.cu)
 void tensor_init(PlanCore& s);

@@ -263,6 +263,7 @@ PlanCore::~PlanCore() {
     cudaFree(d_scale);
     for (auto& sl : pipe) sl.reset();
     tensor_release(*this);
+    wide.reset();
     cudaFree(d_err);
     cudaFree(d_work);
     cudaFree(d_batch_work);
@@ -276,7 +277,8 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     if (!q64 || q_limbs == 0) throw Failure(PM_ERR_INVALID, "q is missing");
     if (n_ < 2 || (n_ & (n_ - 1))) throw Failure(PM_ERR_INVALID, "n must be a power of two >= 2");
     if (n_ > uint32_t(kNMax)) throw Failure(PM_ERR_UNSUPPORTED, "n above 65536");
-    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_SPECIAL_FORM)) throw Failure(PM_ERR_INVALID, "unknown flags");
+    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_SPECIAL_FORM | PM_WIDE_NTT))
+        throw Failure(PM_ERR_INVALID, "unknown flags");
     q.assign(2 * q_limbs, 0);
     for (uint32_t i = 0; i < q_limbs; ++i) {
         q[2 * i] = uint32_t(q64[i]);
@@ -348,6 +350,10 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     }
 
     workspace_bytes = size_t(2) * P * n * sizeof(uint32_t);
+    if (flags & PM_WIDE_NTT) {
+        wide_init(*this);
+        workspace_bytes = std::max(workspace_bytes, wide_workspace_bytes(*this));
+    }
     io_bytes = size_t(n) * coef_limbs * sizeof(uint64_t);
     cuda_check(cudaMalloc(&d_mq, mq.size() * 4), "allocate CRT rows");
     cuda_check(cudaMalloc(&d_consts, consts.size() * 4), "allocate q constants");
@@ -526,7 +532,9 @@ void check_device_pointers(const PlanCore& s, const void* a, const void* b, cons
     for (int i = 0; i < 4; ++i) {
         if (!ptrs[i]) continue;
         const uintptr_t addr = reinterpret_cast<uintptr_t>(ptrs[i]);
-        const uintptr_t need = (s.flags & PM_CONVERT_TENSOR) && i != 2 ? 16 : 8;
+        // tensor path: tensor maps over a, b and the workspace; wide NTT: 16-byte workspace loads
+        const bool tensor = (s.flags & PM_CONVERT_TENSOR) != 0;
+        const uintptr_t need = (tensor && i != 2) || (s.wide && i == 3) ? 16 : 8;
         if (addr % need)
             throw Failure(PM_ERR_INVALID, std::string(names[i]) + " must be " + std::to_string(need) +
                                               "-byte aligned");
@@ -575,7 +583,9 @@ void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint6
         const uint32_t* a32 = reinterpret_cast<const uint32_t*>(a) + z * io_words;
         const uint32_t* b32 = reinterpret_cast<const uint32_t*>(b) + z * io_words;
         uint32_t* c32 = reinterpret_cast<uint32_t*>(c) + z * io_words;
-        if (s.flags & PM_CONVERT_TENSOR)
+        if (s.wide)
+            launch_wide(s, a32, b32, c32, work, g, st);
+        else if (s.flags & PM_CONVERT_TENSOR)
             launch_tensor(s, a32, b32, c32, work, g, st);
         else
             launch_simt(s, a32, b32, c32, work, g, st);

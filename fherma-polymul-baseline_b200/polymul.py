@@ -28,6 +28,7 @@ PM_ERR_BUSY = 6
 PM_CONVERT_SIMT = 0
 PM_CONVERT_TENSOR = 1
 PM_SPECIAL_FORM = 2
+PM_WIDE_NTT = 4
 
 _lib = None
 
@@ -160,7 +161,7 @@ def selftest_bounded_wait(limit_us):
 class Plan:
     """A product plan for (n, q): basis, CRT constants, workspace, staging."""
 
-    def __init__(self, n, q, coef_limbs=None, tensor=False, special_form=False):
+    def __init__(self, n, q, coef_limbs=None, tensor=False, special_form=False, wide=False):
         self.q = int(q)
         qarr = q_limbs_of(self.q)
         self.n = int(n)
@@ -169,7 +170,7 @@ class Plan:
         check(lib().pm_plan_create(ctypes.byref(self._h), self.n,
                                    qarr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(qarr),
                                    self.coef_limbs, (PM_CONVERT_TENSOR if tensor else PM_CONVERT_SIMT)
-                                   | (PM_SPECIAL_FORM if special_form else 0)))
+                                   | (PM_SPECIAL_FORM if special_form else 0) | (PM_WIDE_NTT if wide else 0)))
         info = PlanInfo()
         check(lib().pm_plan_get_info(self._h, ctypes.byref(info)))
         self.info = info

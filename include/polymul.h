@@ -48,7 +48,12 @@ enum pm_flags {
      * quartic/host_setup.h:41-110), reduce the CRT sum by folding 2^k = delta instead of by the
      * general Barrett division.  Same results; ignored for other q.  Measured no faster on
      * B200 (the CRT kernel is bound by latency, not by this step), so it is not the default. */
-    PM_SPECIAL_FORM = 2
+    PM_SPECIAL_FORM = 2,
+    /* The reference's wide backend for comparison (solve.cu): the NTT taken modulo q itself,
+     * each butterfly a W-word Montgomery multiplication, no residues and no CRT.  Needs a
+     * prime q = 1 (mod 2n) (the FHERMA modulus 2^868 - 11993087 is one at n <= 32768);
+     * PM_ERR_UNSUPPORTED otherwise.  Same results as the RNS method, several times slower. */
+    PM_WIDE_NTT = 4
 };
 
 typedef struct {
