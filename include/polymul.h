@@ -118,12 +118,13 @@ int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c
 
 /*
  * A batch of `count` products of one plan, stored back to back: a, b, c are
- * device arrays [count][n][coef_limbs].  The library runs them in groups whose
- * residue planes fit in L2, so the three passes of a group hand their planes
- * to each other on-chip.  workspace: a device buffer of workspace_bytes (at
- * least one product's worth; more allows larger groups, see
- * pm_batch_workspace_size), or NULL to use a plan-owned buffer that the first
- * call allocates.  Asynchronous on `stream`.
+ * device arrays [count][n][coef_limbs].  The library runs them in launch
+ * groups (one launch per pass covers a group; by default up to ~1 GB of residue
+ * planes, 64 products at n = 32768, or the autotuner's choice).  workspace: a
+ * device buffer of workspace_bytes (at least one product's worth; a smaller
+ * buffer than a group needs shrinks the group, see pm_batch_workspace_size), or
+ * NULL to use a plan-owned buffer that the first call allocates.  Asynchronous
+ * on `stream`.
  */
 int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
                       void* workspace, size_t workspace_bytes, pm_stream stream);
