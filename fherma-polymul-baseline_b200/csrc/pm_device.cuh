@@ -218,10 +218,17 @@ __device__ __forceinline__ void exchange_sync(bool warp_local) {
 // sa, sb: 2C words of exchange space; stf, sti: the row's twiddles.
 // Every exchange stores a thread's values back to the very words that thread
 // loaded in the pass (so no barrier is needed before the store), then meets the
-// others before the next pass loads its own layout.
-template <int LOGC, int KP>
+// others before the next pass loads its own layout.  after_last_load() runs on
+// every thread once the last pass has loaded its values (sa and sb are not
+// read again).
+struct NoHook {
+    __device__ void operator()() const {}
+};
+
+template <int LOGC, int KP, class Hook = NoHook>
 __device__ __forceinline__ void row_transform(uint32_t (&va)[8], uint32_t (&vb)[8], uint32_t* sa, uint32_t* sb,
-                                              const uint2* stf, const uint2* sti, int tid, const PrimeConst& pc) {
+                                              const uint2* stf, const uint2* sti, int tid, const PrimeConst& pc,
+                                              Hook after_last_load = Hook{}) {
     constexpr int C = 1 << LOGC;
     constexpr int T = C / 8;
     constexpr int NP = LOGC / KP;   // full passes
@@ -263,6 +270,7 @@ __device__ __forceinline__ void row_transform(uint32_t (&va)[8], uint32_t (&vb)[
     for (int q = NP - 1; q >= 0; --q) {
         const int s0 = KP * q, logd = LOGC - s0 - KP;
         if (q + 1 < NP || REM) pass_load<KP, WL>(va, sa, tid, T, logd);
+        if (q == 0) after_last_load();
         pass_inverse<KP, WL>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
         if (q > 0) {
             pass_store<KP, WL>(va, sa, tid, T, logd);

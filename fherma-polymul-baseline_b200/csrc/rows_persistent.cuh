@@ -7,16 +7,19 @@
 //   - stages the pair's 2C forward/inverse row twiddles with bulk copies, only
 //     when the pair changes (once per pair instead of once per product);
 //   - has the item's two rows (a and b, 4C bytes each) in shared memory already:
-//     they were requested by bulk copy while the previous item was transformed;
-//   - requests the next item's rows into the other buffer, then runs the same
-//     register/shared-memory passes as K2 (row_transform) on this one, using
-//     its own data buffer as the exchange space, and stores the product row.
-// One row per CTA (T = C/8 threads), C >= 1024.  Bulk copies need 16-byte
-// aligned rows: the host launches this kernel only on 16-byte aligned
-// workspaces.
+//     they were requested by bulk copy while the previous item was finishing;
+//   - runs the same register/shared-memory passes as K2 (row_transform) on
+//     them, using the data buffer itself as the exchange space; as soon as
+//     every thread holds the values of the last pass, the buffer is free and
+//     the next item's rows are requested into it, landing while this item's
+//     last stages run and its product row is stored.
+// One data buffer instead of two keeps a CTA at 48 KB (C = 2048), so four CTAs
+// (with at most 64 registers a thread) share an SM.  One row per CTA
+// (T = C/8 threads), C >= 1024.  Bulk copies need 16-byte aligned rows: the
+// host launches this kernel only on 16-byte aligned workspaces.
 //
-// Dynamic shared memory: C uint2 forward and C uint2 inverse twiddles, two data
-// buffers of 2C words, three mbarriers (data 0, data 1, twiddles): 32C + 24 B.
+// Dynamic shared memory: C uint2 forward and C uint2 inverse twiddles, one data
+// buffer of 2C words, two mbarriers (data, twiddles): 24C + 16 B.
 #pragma once
 
 #include <cstdint>
@@ -26,8 +29,8 @@
 
 namespace pm {
 
-constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 3 : 6); }
-constexpr size_t k2p_smem_bytes(int logc) { return (size_t(32) << logc) + 3 * sizeof(uint64_t); }
+constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 4 : 6); }
+constexpr size_t k2p_smem_bytes(int logc) { return (size_t(24) << logc) + 2 * sizeof(uint64_t); }
 
 template <int LOGC, int KP>
 __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
@@ -40,8 +43,8 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
     extern __shared__ __align__(16) uint2 smem2[];
     uint2* stf = smem2;
     uint2* sti = smem2 + C;
-    uint32_t* sd = reinterpret_cast<uint32_t*>(smem2 + 2 * C);  // [2][2C] words
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sd + 4 * C);   // data 0, data 1, twiddles
+    uint32_t* sd = reinterpret_cast<uint32_t*>(smem2 + 2 * C);  // [2C] words
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sd + 2 * C);   // data, twiddles
 
     const int tid = threadIdx.x;
     const int R = 1 << logR;
@@ -51,19 +54,17 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
     if (tid == 0) {
         tc::mbar_init(&bars[0], 1);
         tc::mbar_init(&bars[1], 1);
-        tc::mbar_init(&bars[2], 1);
     }
     tc::fence_smem_async();
     __syncthreads();
 
-    auto issue_rows = [&](int item, int buf) {
+    auto issue_rows = [&](int item) {
         const int pair = item / count, z = item - pair * count;
         const int i = pair >> logR, r = pair & (R - 1);
         const uint32_t* src = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
-        uint32_t* dst = sd + buf * 2 * C;
-        tc::mbar_expect_tx(&bars[buf], 8u * C);
-        tc::bulk_load(dst, src, 4u * C, &bars[buf]);
-        tc::bulk_load(dst + C, src + size_t(P) * n, 4u * C, &bars[buf]);
+        tc::mbar_expect_tx(&bars[0], 8u * C);
+        tc::bulk_load(sd, src, 4u * C, &bars[0]);
+        tc::bulk_load(sd + C, src + size_t(P) * n, 4u * C, &bars[0]);
     };
     // every thread tracks the copies: bit b of `phases` is the parity of barrier
     // b's next completion, bit b of `pending` marks a copy not yet seen complete
@@ -78,42 +79,37 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
         ok = ok && done;
     };
     if (begin < end) {
-        if (tid == 0) issue_rows(begin, 0);
+        if (tid == 0) issue_rows(begin);
         pending |= 1u;
     }
     int cur_pair = -1;
     PrimeConst pc{};
     for (int k = begin; k < end; ++k) {
-        const int buf = (k - begin) & 1;
         const int pair = k / count, z = k - pair * count;
         const int i = pair >> logR, r = pair & (R - 1);
-        if (k + 1 < end) {  // the other buffer's last reader was the previous item
-            if (tid == 0) issue_rows(k + 1, buf ^ 1);
-            pending |= 1u << (buf ^ 1);
-        }
         if (pair != cur_pair) {  // twiddles are free: every thread passed the previous item's barrier
             if (tid == 0) {
                 const uint2* gf = tw_fwd + size_t(i) * kNMax;
                 const uint2* gi = tw_inv + size_t(i) * kNMax;
                 // local entry j = 2^s + i' holds Psi_rev[(R + r) 2^s + i']; stage s > 0 is one
                 // contiguous, 16-byte aligned run of 2^s entries, stage 0 a single entry
-                tc::mbar_expect_tx(&bars[2], 16u * uint32_t(C - 2));
+                tc::mbar_expect_tx(&bars[1], 16u * uint32_t(C - 2));
                 for (int s = 1; s < LOGC; ++s) {
-                    tc::bulk_load(stf + (1 << s), gf + (size_t(R + r) << s), 8u << s, &bars[2]);
-                    tc::bulk_load(sti + (1 << s), gi + (size_t(R + r) << s), 8u << s, &bars[2]);
+                    tc::bulk_load(stf + (1 << s), gf + (size_t(R + r) << s), 8u << s, &bars[1]);
+                    tc::bulk_load(sti + (1 << s), gi + (size_t(R + r) << s), 8u << s, &bars[1]);
                 }
                 stf[1] = __ldg(gf + R + r);
                 sti[1] = __ldg(gi + R + r);
             }
-            pending |= 4u;
+            pending |= 2u;
             pc = pcs[i];
-            wait(2);
+            wait(1);
             __syncthreads();  // entry 1, written by thread 0
             cur_pair = pair;
         }
-        wait(buf);
+        wait(0);
 
-        uint32_t* sa = sd + buf * 2 * C;
+        uint32_t* sa = sd;
         uint32_t* sb = sa + C;
         uint32_t va[8], vb[8];
 #pragma unroll
@@ -127,7 +123,15 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
         // the rows arrived unswizzled and the exchanges store swizzled: every thread
         // has its values before any exchange store lands in this buffer
         __syncthreads();
-        row_transform<LOGC, KP>(va, vb, sa, sb, stf, sti, tid, pc);
+        // once every thread holds the last pass's values, the buffer takes the next item's rows
+        row_transform<LOGC, KP>(va, vb, sa, sb, stf, sti, tid, pc, [&]() {
+            tc::fence_smem_async();
+            __syncthreads();
+            if (k + 1 < end) {
+                if (tid == 0) issue_rows(k + 1);
+                pending |= 1u;
+            }
+        });
         uint32_t* ga = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
 #pragma unroll
         for (int m = 0; m < (8 >> KP); ++m)
@@ -140,7 +144,7 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
     // after a wait gave up (and the loop stopped): copies already requested land
     // before the CTA's shared memory goes away; no new copies were requested
     if (tid == 0) {
-        for (int b = 0; b < 3; ++b)
+        for (int b = 0; b < 2; ++b)
             if (pending & (1u << b)) tc::mbar_wait(&bars[b], (phases >> b) & 1u);
         if (!ok) atomicOr(err, 1u);
     }
