@@ -361,7 +361,13 @@ def run_special(args, torch, polymul, tuning):
     out["speedup"] = out["special_form_products_per_s"] / out["general_reduction_products_per_s"]
     # the direct wide-modulus NTT (PM_WIDE_NTT) on the same prime, for comparison: 64 products
     Bw = min(B, 64)
-    wide = polymul.Plan(n, q, coef_limbs=limbs, wide=True)
+    try:
+        wide = polymul.Plan(n, q, coef_limbs=limbs, wide=True)
+    except polymul.PolymulError as e:  # this prime is 1 mod 2n only up to n = 32768
+        out["wide_ntt"] = f"not applicable at n={n}: {e}"
+        del A, Bv
+        torch.cuda.empty_cache()
+        return out
     Cw = torch.empty_like(A[:Bw])
     st = torch.cuda.Stream()
     wide.multiply_batch(A.data_ptr(), Bv.data_ptr(), Cw.data_ptr(), Bw, stream=st.cuda_stream)

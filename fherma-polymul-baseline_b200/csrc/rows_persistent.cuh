@@ -14,7 +14,7 @@
 //     the next item's rows are requested into it, landing while this item's
 //     last stages run and its product row is stored.
 // One data buffer instead of two keeps a CTA at 48 KB (C = 2048), so four CTAs
-// (with at most 64 registers a thread) share an SM.  One row per CTA
+// (with at most 64 registers a thread) share an SM; at C = 4096, 96 KB and two.  One row per CTA
 // (T = C/8 threads), C >= 1024.  Bulk copies need 16-byte aligned rows: the
 // host launches this kernel only on 16-byte aligned workspaces.
 //
@@ -29,7 +29,7 @@
 
 namespace pm {
 
-constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 1 : (logc >= 11 ? 4 : 6); }
+constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 2 : (logc >= 11 ? 4 : 6); }
 constexpr size_t k2p_smem_bytes(int logc) { return (size_t(24) << logc) + 2 * sizeof(uint64_t); }
 
 template <int LOGC, int KP>
