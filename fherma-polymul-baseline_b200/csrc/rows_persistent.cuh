@@ -29,7 +29,7 @@
 
 namespace pm {
 
-constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 2 : (logc >= 11 ? 4 : 6); }
+constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 2 : (logc >= 11 ? 4 : 8); }
 constexpr size_t k2p_smem_bytes(int logc) { return (size_t(24) << logc) + 2 * sizeof(uint64_t); }
 
 template <int LOGC, int KP>
