@@ -339,8 +339,14 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
             if (cj < np && cc < Gc) {
                 const int ci = it.pg * tc::kConvGroup + cj;
                 uint32_t v[R];
+                const uint32_t* col = sT + cj * kTS + cc;
+                if (Gc == 8) {  // every ring of 128 coefficients or more: constant offsets
 #pragma unroll
-                for (int r = 0; r < R; ++r) v[r] = sT[cj * kTS + r * Gc + cc];
+                    for (int r = 0; r < R; ++r) v[r] = col[r * 8];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) v[r] = col[r * Gc];
+                }
 #pragma unroll
                 for (int s = 0; s < LOGR; ++s) {
                     const int h = R >> (s + 1);
@@ -350,8 +356,9 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
                             ct_bfly(v[r], v[r + h], twr[(1 << s) + (r >> (LOGR - s)) - 1], cpc.p, cpc.two_p);
                 }
                 uint32_t* dst = t.res + (size_t(it.poly) * t.P + ci) * t.n + size_t(it.cg) * Gc + cc;
+                const size_t row = size_t(1) << t.logC;
 #pragma unroll
-                for (int r = 0; r < R; ++r) dst[size_t(r) << t.logC] = v[r];
+                for (int r = 0; r < R; ++r, dst += row) *dst = v[r];
             }
             // sT is rewritten by the next item; a failed wait (or the producer's) ends the loop for all workers
             if (tc::bar_sync_or(1, 128, !ok || s_abort)) break;
