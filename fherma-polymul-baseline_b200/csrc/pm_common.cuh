@@ -29,17 +29,9 @@ __device__ __forceinline__ uint32_t shoup_mul(uint32_t x, uint2 w, uint32_t p) {
 // [0, 2m) -> [0, m); the unsigned min picks x - m exactly when it did not wrap.
 __device__ __forceinline__ uint32_t csub(uint32_t x, uint32_t m) { return min(x, x - m); }
 
-// x mod p for x < 2^60 (Barrett with mu = floor(2^61/p)); quotient error <= 2.
-__device__ __forceinline__ uint32_t reduce60(uint64_t x, uint32_t p, uint32_t mu) {
-    uint32_t xh = uint32_t(x >> 29);
-    uint32_t q = uint32_t((uint64_t(xh) * mu) >> 32);
-    uint32_t r = uint32_t(x) - q * p;
-    r = csub(r, p);
-    return csub(r, p);
-}
-
-// x mod p up to two extra p, for x < 2^60: the quotient estimate of reduce60
-// without its corrections, in [0, 3p) -- enough for a forward butterfly input.
+// x mod p up to two extra p, for x < 2^60: Barrett with mu = floor(2^61/p), whose
+// quotient estimate is at most 2 below floor(x/p), without the two corrections --
+// the result lies in [0, 3p), enough for a forward butterfly input.
 __device__ __forceinline__ uint32_t reduce60_lazy(uint64_t x, uint32_t p, uint32_t mu) {
     const uint32_t q = uint32_t((uint64_t(uint32_t(x >> 29)) * mu) >> 32);
     return uint32_t(x) - q * p;
