@@ -7,7 +7,10 @@
 //   conversion items  (product, prime group, polynomial, column group) ordered
 //                     prime group first -- one persistent launch of k1t_convert;
 //   row items         (product, prime, first row) per ring size class -- one
-//                     launch of k2_rows_items per class;
+//                     launch per class: the persistent k2p_rows for rows of
+//                     1024 values or more (items prime/row first, so a CTA
+//                     stages a row's twiddles once for every product that
+//                     has it), k2_rows_items for shorter rows;
 //   CRT items         (product, column group) per width class -- one persistent
 //                     launch of k3t_crt per class.
 // These launches are captured into a CUDA graph (the classes of a phase on
@@ -24,6 +27,7 @@
 
 #include "../../include/polymul.h"
 #include "pm_internal.h"
+#include "rows_persistent.cuh"
 #include "tensor_kernels.cuh"
 
 namespace pm {
@@ -42,6 +46,21 @@ __global__ void __launch_bounds__(k2_threads(LOGC), k2_min_blocks(LOGC))
     k2_row_body<LOGC, KP>(work + d.ws_off, pcs[it.y], tw_fwd, tw_inv, d.n, logR, d.P, int(it.y), int(it.z) + sub,
                           sub, tid, rows_per_cta);
 }
+
+// rows of one size class from a table of (product, prime, row) items
+struct TableRowWork {
+    const uint4* items;
+    int nitems;
+    const BatchProduct* prod;
+    uint32_t* work;
+    __device__ int total() const { return nitems; }
+    __device__ RowItem item(int k) const {
+        const uint4 v = items[k];
+        const BatchProduct& d = prod[v.x];
+        return RowItem{int(v.y), int(v.z), work + d.ws_off + size_t(v.y) * d.n + (size_t(v.z) << d.logC),
+                       size_t(d.P) * d.n};
+    }
+};
 
 namespace {
 
@@ -78,8 +97,18 @@ CUtensorMap encode(CUtensorMapDataType type, const void* base, const cuuint64_t 
 
 template <int LOGC, int KP>
 void launch_rows_class(const uint4* items, int count, int rows_per_item, const BatchProduct* prod, uint32_t* work,
-                       const DeviceBasis& B, cudaStream_t st) {
+                       const DeviceBasis& B, uint32_t* err, cudaStream_t st) {
     constexpr int C = 1 << LOGC, T = C / 8;
+    if constexpr (LOGC >= 10) {
+        const size_t smem = k2p_smem_bytes(LOGC);
+        cuda_check(cudaFuncSetAttribute(k2p_rows<LOGC, KP, TableRowWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(smem)),
+                   "batch row shared memory");
+        const TableRowWork w{items, count, prod, work};
+        const int ctas = std::min(count, sm_count_dev() * k2p_min_blocks(LOGC));
+        k2p_rows<LOGC, KP, TableRowWork><<<ctas, T, smem, st>>>(w, B.d_pc, B.d_tw_fwd, B.d_tw_inv, 4, err);
+        return;
+    }
     const size_t smem = size_t(rows_per_item) * 24 * C;
     if (smem > 48 * 1024)
         cuda_check(cudaFuncSetAttribute(k2_rows_items<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -91,25 +120,25 @@ void launch_rows_class(const uint4* items, int count, int rows_per_item, const B
 
 template <int LOGC>
 void launch_rows_radix(int radix_log, const uint4* items, int count, int rows, const BatchProduct* prod,
-                       uint32_t* work, const DeviceBasis& B, cudaStream_t st) {
+                       uint32_t* work, const DeviceBasis& B, uint32_t* err, cudaStream_t st) {
     if (radix_log == 2)
-        launch_rows_class<LOGC, 2>(items, count, rows, prod, work, B, st);
+        launch_rows_class<LOGC, 2>(items, count, rows, prod, work, B, err, st);
     else
-        launch_rows_class<LOGC, 3>(items, count, rows, prod, work, B, st);
+        launch_rows_class<LOGC, 3>(items, count, rows, prod, work, B, err, st);
 }
 
 void launch_rows_any(int logC, int radix_log, const uint4* items, int count, int rows, const BatchProduct* prod,
-                     uint32_t* work, const DeviceBasis& B, cudaStream_t st) {
+                     uint32_t* work, const DeviceBasis& B, uint32_t* err, cudaStream_t st) {
     switch (logC) {
-        case 4: return launch_rows_radix<4>(radix_log, items, count, rows, prod, work, B, st);
-        case 5: return launch_rows_radix<5>(radix_log, items, count, rows, prod, work, B, st);
-        case 6: return launch_rows_radix<6>(radix_log, items, count, rows, prod, work, B, st);
-        case 7: return launch_rows_radix<7>(radix_log, items, count, rows, prod, work, B, st);
-        case 8: return launch_rows_radix<8>(radix_log, items, count, rows, prod, work, B, st);
-        case 9: return launch_rows_radix<9>(radix_log, items, count, rows, prod, work, B, st);
-        case 10: return launch_rows_radix<10>(radix_log, items, count, rows, prod, work, B, st);
-        case 11: return launch_rows_radix<11>(radix_log, items, count, rows, prod, work, B, st);
-        case 12: return launch_rows_radix<12>(radix_log, items, count, rows, prod, work, B, st);
+        case 4: return launch_rows_radix<4>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 5: return launch_rows_radix<5>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 6: return launch_rows_radix<6>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 7: return launch_rows_radix<7>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 8: return launch_rows_radix<8>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 9: return launch_rows_radix<9>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 10: return launch_rows_radix<10>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 11: return launch_rows_radix<11>(radix_log, items, count, rows, prod, work, B, err, st);
+        case 12: return launch_rows_radix<12>(radix_log, items, count, rows, prod, work, B, err, st);
         default: throw Failure(PM_ERR_UNSUPPORTED, "row size outside the batch kernels");
     }
 }
@@ -210,7 +239,8 @@ struct BatchCore {
         for (size_t k = 0; k < row_classes.size(); ++k) {
             const RowClass& rc = row_classes[k];
             cudaStream_t s = fork(k);
-            launch_rows_any(rc.logC, rc.radix_log, d_row_items + rc.offset, rc.count, rc.rows, d_prod, d_work, B, s);
+            launch_rows_any(rc.logC, rc.radix_log, d_row_items + rc.offset, rc.count, rc.rows, d_prod, d_work, B, d_err,
+                            s);
             used.push_back(s);
         }
         for (size_t k = 0; k < used.size(); ++k) join(used[k], k);
@@ -309,6 +339,10 @@ struct BatchCore {
         }
         std::vector<uint4> row_items;
         for (auto& [logC, items] : rows_by_c) {
+            if (logC >= 10)  // the persistent row kernel: consecutive items share a (prime, row) pair
+                std::stable_sort(items.begin(), items.end(), [](const uint4& x, const uint4& y) {
+                    return x.y != y.y ? x.y < y.y : x.z < y.z;
+                });
             // the radix the autotuner picked for plans of this row size, radix-8 by default
             int radix_log = 3;
             for (auto& p : plans)

@@ -433,15 +433,15 @@ void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStr
         // bulk copies need 16-byte aligned rows (n, C and the product stride are multiples of 4 words)
         if (s.tune.row_persistent && (reinterpret_cast<uintptr_t>(work) & 15) == 0 && (bt.ws_bstride & 3) == 0) {
             const size_t smem = k2p_smem_bytes(LOGC);
-            cuda_check(cudaFuncSetAttribute(k2p_rows<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cuda_check(cudaFuncSetAttribute(k2p_rows<LOGC, KP, PlanRowWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             int(smem)),
                        "raise K2P shared memory");
             const int64_t items = int64_t(s.P) << s.logR;
             const int64_t total = items * bt.count;
             const int ctas = int(std::min<int64_t>(total, int64_t(s.sms) * k2p_min_blocks(LOGC)));
-            k2p_rows<LOGC, KP><<<ctas, T, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
-                                                      int(s.n), int(s.logR), int(s.P), int(bt.count),
-                                                      bt.ws_bstride, s.d_err);
+            const PlanRowWork w{work, bt.ws_bstride, int(s.n), int(s.logR), int(s.logC), int(s.P), int(bt.count)};
+            k2p_rows<LOGC, KP, PlanRowWork><<<ctas, T, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_fwd,
+                                                                   s.basis->d_tw_inv, int(s.logR), s.d_err);
             return;
         }
     }

@@ -1,8 +1,11 @@
 // K2P: the row stages of K2 as a persistent kernel.
 //
-// Work items are (prime i, row r, product z) of one launch group, numbered
-// pair-major (pair = i * R + r, item = pair * count + z), so the items a CTA
-// takes in a row share their twiddles.  Each CTA owns a contiguous range of
+// Work items are (prime i, row r, product z), numbered pair-major (all
+// products of a (prime, row) pair in a row), so the items a CTA takes in a row
+// share their twiddles.  A work source says how many items there are and
+// where each one's rows live: PlanRowWork computes them for `count` products
+// of one plan (pair = i * R + r, item = pair * count + z); a batch of products
+// of one row size but different q reads them from a table.  Each CTA owns a contiguous range of
 // items and, for each of them:
 //   - stages the pair's 2C forward/inverse row twiddles with bulk copies, only
 //     when the pair changes (once per pair instead of once per product);
@@ -29,14 +32,32 @@
 
 namespace pm {
 
+// One row item: prime i, row r, the row of a (C words) and the distance to b's.
+struct RowItem {
+    int i, r;
+    uint32_t* a;
+    size_t b_off;
+};
+
+struct PlanRowWork {
+    uint32_t* res;  // residue planes of product 0; product z at res + z * ws_bstride
+    size_t ws_bstride;
+    int n, logR, logC, P, count;
+    __device__ int total() const { return (P << logR) * count; }
+    __device__ RowItem item(int k) const {
+        const int pair = k / count, z = k - pair * count;
+        const int i = pair >> logR, r = pair & ((1 << logR) - 1);
+        return RowItem{i, r, res + size_t(z) * ws_bstride + size_t(i) * n + (size_t(r) << logC), size_t(P) * n};
+    }
+};
+
 constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 2 : (logc >= 11 ? 4 : 8); }
 constexpr size_t k2p_smem_bytes(int logc) { return (size_t(24) << logc) + 2 * sizeof(uint64_t); }
 
-template <int LOGC, int KP>
+template <int LOGC, int KP, class Work>
 __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
-    k2p_rows(uint32_t* __restrict__ res, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
-             const uint2* __restrict__ tw_inv, int n, int logR, int P, int count, size_t ws_bstride,
-             uint32_t* __restrict__ err) {
+    k2p_rows(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
+             const uint2* __restrict__ tw_inv, int logR, uint32_t* __restrict__ err) {
     constexpr int C = 1 << LOGC, T = C / 8;
     constexpr int logd0 = LOGC - KP;  // first pass: s0 = 0
     static_assert(LOGC >= 10, "one row per CTA needs C >= 1024");
@@ -48,7 +69,7 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
 
     const int tid = threadIdx.x;
     const int R = 1 << logR;
-    const int total = P * R * count;
+    const int total = w.total();
     const int begin = int(int64_t(blockIdx.x) * total / gridDim.x);
     const int end = int(int64_t(blockIdx.x + 1) * total / gridDim.x);
     if (tid == 0) {
@@ -58,13 +79,11 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
     tc::fence_smem_async();
     __syncthreads();
 
-    auto issue_rows = [&](int item) {
-        const int pair = item / count, z = item - pair * count;
-        const int i = pair >> logR, r = pair & (R - 1);
-        const uint32_t* src = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
+    auto issue_rows = [&](int k) {
+        const RowItem it = w.item(k);
         tc::mbar_expect_tx(&bars[0], 8u * C);
-        tc::bulk_load(sd, src, 4u * C, &bars[0]);
-        tc::bulk_load(sd + C, src + size_t(P) * n, 4u * C, &bars[0]);
+        tc::bulk_load(sd, it.a, 4u * C, &bars[0]);
+        tc::bulk_load(sd + C, it.a + it.b_off, 4u * C, &bars[0]);
     };
     // every thread tracks the copies: bit b of `phases` is the parity of barrier
     // b's next completion, bit b of `pending` marks a copy not yet seen complete
@@ -85,8 +104,8 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
     int cur_pair = -1;
     PrimeConst pc{};
     for (int k = begin; k < end; ++k) {
-        const int pair = k / count, z = k - pair * count;
-        const int i = pair >> logR, r = pair & (R - 1);
+        const RowItem it = w.item(k);
+        const int i = it.i, r = it.r, pair = i * R + r;
         if (pair != cur_pair) {  // twiddles are free: every thread passed the previous item's barrier
             if (tid == 0) {
                 const uint2* gf = tw_fwd + size_t(i) * kNMax;
@@ -132,7 +151,7 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
                 pending |= 1u;
             }
         });
-        uint32_t* ga = res + size_t(z) * ws_bstride + size_t(i) * n + size_t(r) * C;
+        uint32_t* ga = it.a;
 #pragma unroll
         for (int m = 0; m < (8 >> KP); ++m)
 #pragma unroll
