@@ -149,7 +149,7 @@ void launch_crt_class(const TableCrtWork& w, int ctas, const DeviceBasis& B, uin
     cuda_check(cudaFuncSetAttribute(k3t_crt<4, W, TableCrtWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(smem)),
                "batch CRT shared memory");
-    k3t_crt<4, W, TableCrtWork><<<ctas, 128, smem, st>>>(w, B.d_pc, B.d_tw_inv, err);
+    k3t_crt<4, W, TableCrtWork><<<ctas, tc::kCrtThreads, smem, st>>>(w, B.d_pc, B.d_tw_inv, err);
 }
 
 void launch_crt_any(int W, const TableCrtWork& w, int ctas, const DeviceBasis& B, uint32_t* err, cudaStream_t st) {

@@ -201,7 +201,7 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     w.P = int(s.P);
     w.stride = int(s.stride);
     w.count = int(count);
-    kernel<<<ctas, 128, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_inv, s.d_err);
+    kernel<<<ctas, tc::kCrtThreads, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_inv, s.d_err);
 }
 
 template <int LOGR>

@@ -39,6 +39,7 @@ constexpr int kConvN = 4 * kConvGroup;
 constexpr int kCrtN = 128;      // value bytes + 8 quotient bytes (+ pad)
 constexpr int kCrtK = 256;      // 4 bytes per prime, 64 primes
 constexpr int kMaxPrimes = 64;
+constexpr int kCrtThreads = 256;  // K3T: 8 warps for the digit phase, warps 0-3 for the epilogue
 }  // namespace tc
 
 struct ConvItem {
@@ -375,7 +376,10 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
 }
 
 // ---------------------------------------------------------------------------
-// K3T: inverse column stages + CRT on the tensor cores, persistent.  Block 128.
+// K3T: inverse column stages + CRT on the tensor cores, persistent.  Block of
+// kCrtThreads = 256: all eight warps run the digit phase (the column stages of
+// the tile's (prime, column) pairs), warps 0-3 (the owners of the 128 TMEM
+// lanes) the per-coefficient epilogue.
 // An item's residues for every prime arrive by TMA (box: Gc columns x P primes x
 // R rows of u32, landing as [row][prime][column], so the 4 primes x 8 columns a
 // warp reads per row fall in 32 distinct banks); the next item's box is
@@ -389,7 +393,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
 // residue box 64*R*8 words, inverse column twiddles 64*(R-1) uint2.
 // ---------------------------------------------------------------------------
 template <int LOGR, int W, class Work, int RED = kReduceEither>
-__global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs,
+__global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs,
                                                const uint2* __restrict__ tw_inv, uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
     constexpr int RT = R > 1 ? R - 1 : 1;
@@ -410,7 +414,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
     const int begin = int(blockIdx.x) * chunk;
     const int end = min(total, begin + chunk);
 
-    for (int k = tid; k < 2048; k += 128) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
+    for (int k = tid; k < 2048; k += tc::kCrtThreads) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
     if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
     if (tid == 0) {
         tc::mbar_init(&tma_bar, 1);
@@ -444,13 +448,13 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         const int cg = it.y;
         if (t.crt_w != cur_w || t.P != cur_P) {  // the previous item's MMA is complete: B may be rewritten
             const uint4* src = reinterpret_cast<const uint4*>(t.crt_w);
-            for (int q = tid; q < 2048; q += 128) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
-            for (int q = tid; q < 2 * W; q += 128) s_q[q] = t.consts[q];
+            for (int q = tid; q < 2048; q += tc::kCrtThreads) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
+            for (int q = tid; q < 2 * W; q += tc::kCrtThreads) s_q[q] = t.consts[q];
             if (R > 1)
-                for (int q = tid; q < t.P * RT; q += 128)
+                for (int q = tid; q < t.P * RT; q += tc::kCrtThreads)
                     sTw[q] = __ldg(tw_inv + size_t(q / RT) * kNMax + 1 + q % RT);
             if (t.P != cur_P)  // K columns of absent primes must read as zero
-                for (int q = tid; q < 2048; q += 128) reinterpret_cast<uint4*>(sA)[q] = make_uint4(0, 0, 0, 0);
+                for (int q = tid; q < 2048; q += tc::kCrtThreads) reinterpret_cast<uint4*>(sA)[q] = make_uint4(0, 0, 0, 0);
             cur_w = t.crt_w;
             cur_P = t.P;
             tc::fence_smem_async();
@@ -461,7 +465,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
             tma_phase ^= 1;
         } else {
             const int box = t.P * R * Gc;
-            for (int q = tid; q < box; q += 128) {
+            for (int q = tid; q < box; q += tc::kCrtThreads) {
                 const int c = q % Gc, i = (q / Gc) % t.P, r = q / (Gc * t.P);
                 sR[q] = t.work[size_t(i) * t.n + (size_t(r) << t.logC) + size_t(cg) * Gc + c];
             }
@@ -469,7 +473,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         }
         // --- inverse column stages and CRT digits into A ---
         const int pairs = t.P * Gc;
-        for (int pr = tid; pr < pairs; pr += 128) {
+        for (int pr = tid; pr < pairs; pr += tc::kCrtThreads) {
             const int i = pr / Gc, c = pr - i * Gc;
             const PrimeConst pc = pcs[i];
             uint32_t v[R];
@@ -522,8 +526,9 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
         mma_phase ^= 1;
         tc::fence_after();
-        // --- carry-propagate the byte columns of row m = tid ---
+        // --- carry-propagate the byte columns of row m = tid (warps 0-3, the TMEM lane owners) ---
         // value: NV/4 = W+1 words plus the carry-out; quotient estimate: 8 columns
+        if (warp < 4) {
         uint32_t acc[W + 2];
         uint64_t carry = 0;
         uint64_t fsum0 = 0, fsum1 = 0;
@@ -556,6 +561,7 @@ __global__ void __launch_bounds__(128) k3t_crt(const __grid_constant__ Work w, c
         if (rr < R) {
             const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
             crt_finish<W, RED>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride);
+        }
         }
         tc::fence_before();
         __syncthreads();
