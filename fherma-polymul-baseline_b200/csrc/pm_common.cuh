@@ -37,6 +37,16 @@ __device__ __forceinline__ uint32_t reduce60_lazy(uint64_t x, uint32_t p, uint32
     return uint32_t(x) - q * p;
 }
 
+// (hi 2^16 + lo) mod p up to two extra p, for hi < 2^32 - 2^16, any 32-bit lo
+// and m = floor(2^48 / p), without forming the 48-bit value: u = hi + (lo >> 16)
+// is its top part, u 2^16 <= v < u 2^16 + 2^16, and q = floor(u m / 2^32)
+// satisfies v/p - 2 - 2^16/p < q <= v/p, so v - q p lies in [0, 3p) and is
+// exact in 32-bit arithmetic.
+__device__ __forceinline__ uint32_t reduce48_lazy(uint32_t lo, uint32_t hi, uint32_t p, uint32_t m) {
+    const uint32_t q = __umulhi(hi + (lo >> 16), m);
+    return lo + (hi << 16) - q * p;
+}
+
 // x * y * 2^-32 mod p up to one extra p, for x, y in [0, 2p): result in (0, 2p).
 // Montgomery reduction with m = lo(xy) p^-1: xy - m p is a multiple of 2^32 and,
 // as xy < 4p^2 < p 2^32, (xy - m p) / 2^32 lies in (-p, p).

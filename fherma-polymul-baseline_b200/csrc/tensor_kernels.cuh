@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
     __shared__ uint64_t tma_full[2], mma_full[2], tmem_empty[2], b_full;
     __shared__ uint32_t tmem_base;
     __shared__ volatile uint32_t s_abort;
-    __shared__ PrimeConst spc[tc::kConvGroup];
+    __shared__ uint2 spm[tc::kConvGroup];  // the group's primes and floor(2^48 / p)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int total = w.total();
@@ -303,8 +303,11 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
             const ConvTarget t = w.target(it.z, it.poly);
             const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
             const int buf = kk & 1;
-            if (it.pg != cur_pg) {  // the previous item's closing barrier ended every read of spc
-                if (tid < tc::kConvGroup) spc[tid] = pcs[it.pg * tc::kConvGroup + tid];
+            if (it.pg != cur_pg) {  // the previous item's closing barrier ended every read of spm
+                if (tid < tc::kConvGroup) {
+                    const PrimeConst g = pcs[it.pg * tc::kConvGroup + tid];
+                    spm[tid] = make_uint2(g.p, g.mu >> 13);  // floor(floor(2^61 / p) / 2^13)
+                }
                 const int ci = it.pg * tc::kConvGroup + cj;
 #pragma unroll
                 for (int q = 1; q < R; ++q) twr[q - 1] = __ldg(tw_fwd + size_t(ci) * kNMax + q);
@@ -317,8 +320,8 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
             ph_mma ^= 1u << buf;
             tc::fence_after();
             // --- residues of row m = tid for the group's 16 primes ---
-            // byte-plane sums d_a <= 128 * 255^2 < 2^23, so d0 + 2^8 d1 and d2 + 2^8 d3
-            // fit 32 bits and the residue input is (d2 + 2^8 d3) 2^16 + d0 + 2^8 d1 < 2^48
+            // byte-plane sums d_a <= 128 * 255^2 < 2^23, so lo = d0 + 2^8 d1 and hi = d2 + 2^8 d3
+            // are below 2^31.01 and the residue input is hi 2^16 + lo
 #pragma unroll
             for (int q4 = 0; q4 < 4; ++q4) {
                 uint32_t d[16];
@@ -329,8 +332,8 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
                     const int j = 4 * q4 + u;
                     const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
                     const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
-                    const uint64_t v = (uint64_t(hi) << 16) + lo;
-                    sT[j * kTS + tid] = reduce60_lazy(v, spc[j].p, spc[j].mu);  // [0, 3p): butterfly input
+                    const uint2 pm = spm[j];
+                    sT[j * kTS + tid] = reduce48_lazy(lo, hi, pm.x, pm.y);  // [0, 3p): butterfly input
                 }
             }
             tc::fence_before();
