@@ -197,7 +197,7 @@ struct BatchCore {
     cudaGraphExec_t graph = nullptr;
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> events;
-    int conv_ctas_per_sm = 4, crt_ctas_per_sm = 2;  // persistent grid sizes (autotuned)
+    int conv_ctas_per_sm = 3, crt_ctas_per_sm = 2;  // persistent grid sizes (autotuned)
 
     ~BatchCore() {
         cudaSetDevice(device);
@@ -441,7 +441,7 @@ struct BatchCore {
             const int old = rc.radix_log;
             attempt([&] { rc.radix_log = old == 3 ? 2 : 3; }, [&] { rc.radix_log = old; });
         }
-        for (int k : {2, 3}) {
+        for (int k : {2, 3, 4}) {
             const int old = conv_ctas_per_sm;
             if (k == old) continue;
             attempt([&] { conv_ctas_per_sm = k; }, [&] { conv_ctas_per_sm = old; });

@@ -165,9 +165,11 @@ struct TableCrtWork {
 // N=64, K=32) into that accumulator, commit; once the MMA is complete its A tile
 // takes the TMA of the item two ahead.
 // Workers: wait for the item's MMA, tcgen05.ld -> two 32-bit partial sums ->
-// Barrett -> padded transpose, release the accumulator (mbarrier arrival), then
-// 4 forward column stages in registers -> residue planes.  Only the workers
-// meet at (named) barriers, so the producer's waits never hold them.
+// lazy Barrett (the group's primes and factors held in registers: 128 registers
+// a thread at R = 16, three CTAs per SM) -> padded transpose, release the
+// accumulator (mbarrier arrival), then 4 forward column stages in registers ->
+// residue planes.  Only the workers meet at (named) barriers, so the producer's
+// waits never hold them.
 // Barriers: tma_full[2], mma_full[2], tmem_empty[2] (128 arrivals), b_full.
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose
 // 16 x kTS words (kTS = 136: the four primes a warp reads per row sit 8 banks
@@ -294,6 +296,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
         // column-stage role: prime j of the group, column c of the tile
         const int cj = tid / 8, cc = tid % 8;
         uint2 twr[R > 1 ? R - 1 : 1];
+        uint2 rpm[tc::kConvGroup];  // the group's primes and floor(2^48 / p)
         PrimeConst cpc{};
         int cur_pg = -1;
         uint32_t ph_mma = 0;
@@ -314,6 +317,8 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
                 cpc = pcs[ci];
                 cur_pg = it.pg;
                 tc::bar_sync(1, 128);
+#pragma unroll
+                for (int j = 0; j < tc::kConvGroup; ++j) rpm[j] = spm[j];
             }
             const int np = min(tc::kConvGroup, t.P - it.pg * tc::kConvGroup);
             ok = tc::mbar_wait(&mma_full[buf], (ph_mma >> buf) & 1u) && ok;
@@ -332,8 +337,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
                     const int j = 4 * q4 + u;
                     const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
                     const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
-                    const uint2 pm = spm[j];
-                    sT[j * kTS + tid] = reduce48_lazy(lo, hi, pm.x, pm.y);  // [0, 3p): butterfly input
+                    sT[j * kTS + tid] = reduce48_lazy(lo, hi, rpm[j].x, rpm[j].y);  // [0, 3p): butterfly input
                 }
             }
             tc::fence_before();
