@@ -413,17 +413,18 @@ static __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeCons
 template <int W>
 __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q, uint64_t mu_q,
                                              int sbits) {
-    // X = floor(v / 2^(sbits-1)) < 2^38; only words W-4 .. W+1 can hold it
-    const int sh = sbits - 1;
+    // X = floor(v / 2^(sbits-26)) < 2^63; only words W-5 .. W+1 can hold it
+    const int sh = sbits - 26;
     uint64_t X = 0;
 #pragma unroll
-    for (int k = (W >= 4 ? W - 4 : 0); k < W + 2; ++k) {
+    for (int k = (W >= 5 ? W - 5 : 0); k < W + 2; ++k) {
         const int pos = 32 * k - sh;  // bit position of word k inside X
         if (pos > -32 && pos < 64) X |= pos >= 0 ? uint64_t(v[k]) << pos : uint64_t(v[k]) >> (-pos);
     }
-    // quotient estimate, at most 2 below floor(v / q)
-    const uint64_t hi = __umul64hi(X, mu_q), lo = X * mu_q;
-    const uint64_t Q = (hi << 1) | (lo >> 63);
+    // Q = floor(X mu_q / 2^88) <= v / q, and v/q - X mu_q / 2^88 is below
+    // 2^(sbits+62) / q / 2^88 (the floor in X; q > 2^(sbits-1)) + X / 2^88 (the
+    // floor in mu_q), each under 2^-25: Q is at most 1 below floor(v / q)
+    const uint64_t Q = __umul64hi(X, mu_q) >> 24;
     uint32_t qw[W];
 #pragma unroll
     for (int k = 0; k < W; ++k) qw[k] = q[k];
@@ -434,19 +435,16 @@ __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_
     crt_mac<W>(u, uint32_t(Q >> 32), qw);  // high bits (< 2^6) times q, subtracted one word up
     mp_sub<W + 2>(v, t);
     mp_sub_hi<W>(v, u);
-    // [0, 3q) -> [0, q)
+    // [0, 2q) -> [0, q)
     uint32_t qq[W + 2];
 #pragma unroll
     for (int k = 0; k < W + 2; ++k) qq[k] = k < W ? qw[k] : 0u;
+    uint32_t d[W + 2];
 #pragma unroll
-    for (int rep = 0; rep < 2; ++rep) {
-        uint32_t d[W + 2];
+    for (int k = 0; k < W + 2; ++k) d[k] = v[k];
+    const uint32_t borrowed = mp_sub<W + 2>(d, qq);
 #pragma unroll
-        for (int k = 0; k < W + 2; ++k) d[k] = v[k];
-        const uint32_t borrowed = mp_sub<W + 2>(d, qq);
-#pragma unroll
-        for (int k = 0; k < W + 2; ++k) v[k] = borrowed ? v[k] : d[k];
-    }
+    for (int k = 0; k < W + 2; ++k) v[k] = borrowed ? v[k] : d[k];
 }
 
 // v mod q for a special-form q = 2^k - delta (k = sbits >= 80, delta < 2^32;
