@@ -625,7 +625,7 @@ def run_ours(args):
         plan.set_tuning(group=args.group)
         tuning = {"group": args.group, "source": "--group"}
     elif args.autotune:
-        tuning = plan.autotune(reps=3)
+        tuning = plan.autotune(reps=8)
     B = args.batch
     A = device_inputs(torch, B, n, limbs, q, args.seed + 17 + 1000 * rank)
     Bv = device_inputs(torch, B, n, limbs, q, args.seed + 29 + 1000 * rank)
