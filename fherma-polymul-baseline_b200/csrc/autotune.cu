@@ -2,8 +2,9 @@
 // workload (a batch of synthetic products on the plan's device).
 //
 // Knobs (Tuning in pm_internal.h):
-//   row_radix_log    K2 register passes of radix 4 or 8 (more passes with less
-//                    register state, or fewer shared-memory exchanges);
+//   row_radix_log    K2 register passes of radix 4, 8 or 16 (more passes with
+//                    less register state, or fewer shared-memory exchanges;
+//                    radix 16 in the persistent kernel, rows of >= 1024 values);
 //   conv_ctas_per_sm persistent CTAs of the tensor conversion per SM;
 //   crt_ctas_per_sm  persistent CTAs of the tensor CRT per SM;
 //   row_persistent   K2 as one CTA per row, or as the persistent kernel that
@@ -112,7 +113,8 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
         consider(t);
     }
     if (s.logC >= 4) {
-        for (int radix : {2, 3}) {
+        for (int radix : {2, 3, 4}) {
+            if (radix == 4 && !(s.logC >= 10 && best.row_persistent)) continue;  // radix-16: persistent kernel only
             Tuning t = best;
             t.row_radix_log = radix;
             if (radix != best.row_radix_log) consider(t);
@@ -173,13 +175,14 @@ extern "C" int pm_plan_autotune(pm_plan* plan, uint32_t reps, pm_tuning* chosen)
 
 extern "C" int pm_plan_set_tuning(pm_plan* plan, const pm_tuning* t) {
     if (!plan || !t) return pm::fail(PM_ERR_INVALID, "NULL argument");
-    if (t->row_radix != 4 && t->row_radix != 8) return pm::fail(PM_ERR_INVALID, "row_radix must be 4 or 8");
+    if (t->row_radix != 4 && t->row_radix != 8 && t->row_radix != 16)
+        return pm::fail(PM_ERR_INVALID, "row_radix must be 4, 8 or 16");
     if (t->conv_ctas_per_sm < 1 || t->conv_ctas_per_sm > 8 || t->crt_ctas_per_sm < 1 || t->crt_ctas_per_sm > 4)
         return pm::fail(PM_ERR_INVALID, "CTAs per SM out of range");
     if (t->group > 64) return pm::fail(PM_ERR_INVALID, "group above 64");
     if (t->row_persistent > 1) return pm::fail(PM_ERR_INVALID, "row_persistent must be 0 or 1");
     pm::Tuning& u = plan->core.tune;
-    u.row_radix_log = t->row_radix == 4 ? 2 : 3;
+    u.row_radix_log = t->row_radix == 4 ? 2 : (t->row_radix == 8 ? 3 : 4);
     u.conv_ctas_per_sm = int(t->conv_ctas_per_sm);
     u.crt_ctas_per_sm = int(t->crt_ctas_per_sm);
     u.group = t->group;

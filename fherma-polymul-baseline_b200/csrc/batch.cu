@@ -106,16 +106,17 @@ void launch_rows_class(const uint4* items, int count, int rows_per_item, const B
                    "batch row shared memory");
         const TableRowWork w{items, count, prod, work};
         const int ctas = std::min(count, sm_count_dev() * k2p_min_blocks(LOGC));
-        k2p_rows<LOGC, KP, TableRowWork><<<ctas, T, smem, st>>>(w, B.d_pc, B.d_tw_fwd, B.d_tw_inv, 4, err);
-        return;
+        k2p_rows<LOGC, KP, TableRowWork><<<ctas, k2p_threads(LOGC, KP), smem, st>>>(w, B.d_pc, B.d_tw_fwd,
+                                                                                    B.d_tw_inv, 4, err);
+    } else {
+        const size_t smem = size_t(rows_per_item) * 24 * C;
+        if (smem > 48 * 1024)
+            cuda_check(cudaFuncSetAttribute(k2_rows_items<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(smem)),
+                       "batch row shared memory");
+        k2_rows_items<LOGC, KP><<<count, rows_per_item * T, smem, st>>>(items, prod, work, B.d_pc, B.d_tw_fwd,
+                                                                        B.d_tw_inv, 4);
     }
-    const size_t smem = size_t(rows_per_item) * 24 * C;
-    if (smem > 48 * 1024)
-        cuda_check(cudaFuncSetAttribute(k2_rows_items<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(smem)),
-                   "batch row shared memory");
-    k2_rows_items<LOGC, KP><<<count, rows_per_item * T, smem, st>>>(items, prod, work, B.d_pc, B.d_tw_fwd, B.d_tw_inv,
-                                                                    4);
 }
 
 template <int LOGC>
@@ -123,6 +124,8 @@ void launch_rows_radix(int radix_log, const uint4* items, int count, int rows, c
                        uint32_t* work, const DeviceBasis& B, uint32_t* err, cudaStream_t st) {
     if (radix_log == 2)
         launch_rows_class<LOGC, 2>(items, count, rows, prod, work, B, err, st);
+    else if (LOGC >= 10 && radix_log == 4)  // radix-16 passes: the persistent kernel only
+        launch_rows_class<LOGC, LOGC >= 10 ? 4 : 3>(items, count, rows, prod, work, B, err, st);
     else
         launch_rows_class<LOGC, 3>(items, count, rows, prod, work, B, err, st);
 }

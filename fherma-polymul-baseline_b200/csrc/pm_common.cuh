@@ -72,16 +72,17 @@ __device__ __forceinline__ void gs_bfly(uint32_t& x, uint32_t& y, uint2 w, uint3
     y = shoup_mul(d, w, p);
 }
 
-// Shared-memory swizzle: index bits 5, 6 and 7 flip the bank bits {0, 2},
-// {1, 3} and {0, 1, 4}.  Only bits 0..4 change, as a function of bits that do
-// not, so it maps every aligned power-of-two range onto itself and is linear
-// over GF(2).  With it the 32 lanes of a warp reach 32 distinct banks in every
-// pass layout of the row kernels at C = 1024..4096 (radix-8 passes at stride
-// 2^logd, and the closing radix-2/4 pass at stride 1, whose per-access element
-// bits sit in bits 0..1 and need a lane bit XORed into them).
+// Shared-memory swizzle: index bits 5, 6, 7 and 8 flip the bank bits {0, 2},
+// {1, 3}, {0, 1, 4} and {0, 2, 3, 4}.  Only bits 0..4 change, as a function of
+// bits that do not, so it maps every aligned power-of-two range onto itself and
+// is linear over GF(2).  With it the 32 lanes of a warp reach 32 distinct banks
+// in every pass layout of the row kernels at C = 1024..4096, with 8 or 16
+// values a thread (passes at stride 2^logd, and the closing pass at stride 1,
+// whose per-access element bits sit in the low bits and need lane bits XORed
+// into them).
 __device__ __forceinline__ int swz(int idx) {
     const int x = (idx >> 5) & 3;
-    return idx ^ x ^ (x << 2) ^ (((idx >> 7) & 1) * 19);
+    return idx ^ x ^ (x << 2) ^ (((idx >> 7) & 1) * 19) ^ (((idx >> 8) & 1) * 29);
 }
 
 }  // namespace pm

@@ -96,38 +96,39 @@ __global__ void __launch_bounds__(256) k1_convert_cols(const uint32_t* __restric
 
 // ---------------------------------------------------------------------------
 // K2: row stages.  Element mapping of a pass over stages s0..s0+K-1 of a row
-// of C = 2^LOGC values, 8 values per thread, T = C/8 threads per row:
-//   d = C >> (s0+K); for group m < 8>>K: gid = pass_gid(tid, m), blk = gid / d,
+// of C = 2^LOGC values, V = 2^LV values per thread (LV = 3, or 4 for the
+// radix-16 passes of the persistent row kernel), T = C/V threads per row:
+//   d = C >> (s0+K); for group m < V>>K: gid = pass_gid(tid, m), blk = gid / d,
 //   o = gid % d; value l of the group sits at blk*(d<<K) + o + l*d.
 // Twiddle of row stage s = s0+u for the value pair starting at l: the row-local
 // table entry 2^s + blk*2^u + (l >> (K-u)), which holds
 //   Psi_rev[(R + r) * 2^s + blk * 2^u + (l >> (K-u))].
 //
-// Warp-local exchanges (WL: radix-8 passes, T >= 32).  In a radix-8 pass
+// Warp-local exchanges (WL: passes of K = LV stages, T >= 32).  In such a pass
 // (one group, gid = tid) with d <= 32, warp w's values are exactly the words
-// [256w, 256w + 256) (the swizzle keeps bits 8 and up).  The closing pass of
-// K < 3 stages (d = 1) gets the same property by numbering its 8>>K groups
-// so that warp w owns gids [w 2^(8-K), (w+1) 2^(8-K)).  An exchange between
-// two such passes is then a warp's own business: __syncwarp instead of a CTA
-// barrier.
+// [32V w, 32V (w + 1)) (the swizzle keeps bits 5 and up).  The closing pass of
+// K < LV stages (d = 1) gets the same property by numbering its V>>K groups
+// so that warp w owns gids [w 2^(LV+5-K), (w+1) 2^(LV+5-K)).  An exchange
+// between two such passes is then a warp's own business: __syncwarp instead
+// of a CTA barrier.
 // ---------------------------------------------------------------------------
-template <int K, bool WL>
+template <int K, bool WL, int LV = 3>
 __device__ __forceinline__ int pass_gid(int tid, int T, int m) {
-    if constexpr (WL && K < 3)
-        return ((tid >> 5) << (8 - K)) + (m << 5) + (tid & 31);
+    if constexpr (WL && K < LV)
+        return ((tid >> 5) << (LV + 5 - K)) + (m << 5) + (tid & 31);
     else
         return tid + T * m;
 }
 
-// true when a pass of K stages at stride d = 2^logd keeps each warp inside its 256 words
-template <int K, bool WL>
+// true when a pass of K stages at stride d = 2^logd keeps each warp inside its 32V words
+template <int K, bool WL, int LV = 3>
 __host__ __device__ constexpr bool pass_warp_local(int logd) {
-    return WL && (K == 3 ? logd <= 5 : logd == 0);
+    return WL && (K == LV ? logd <= 5 : logd == 0);
 }
 
-template <int K, bool WL = false>
+template <int K, bool WL = false, int LV = 3>
 __device__ __forceinline__ int pass_index(int tid, int T, int m, int l, int logd) {
-    const int gid = pass_gid<K, WL>(tid, T, m);
+    const int gid = pass_gid<K, WL, LV>(tid, T, m);
     const int blk = gid >> logd;
     const int o = gid & ((1 << logd) - 1);
     return (blk << (logd + K)) + o + (l << logd);
@@ -136,40 +137,40 @@ __device__ __forceinline__ int pass_index(int tid, int T, int m, int l, int logd
 // A pass index is a disjoint OR of thread bits (blk, o) and element bits (l),
 // and swz is linear over GF(2), so swz(idx) = swz(thread part) ^ swz(l << logd):
 // one XOR with a constant per access.
-template <int K, bool WL>
+template <int K, bool WL, int LV>
 __device__ __forceinline__ int pass_thread_base(int tid, int T, int m, int logd) {
-    const int gid = pass_gid<K, WL>(tid, T, m);
+    const int gid = pass_gid<K, WL, LV>(tid, T, m);
     const int blk = gid >> logd;
     const int o = gid & ((1 << logd) - 1);
     return swz((blk << (logd + K)) | o);
 }
 
-template <int K, bool WL>
-__device__ __forceinline__ void pass_store(const uint32_t (&v)[8], uint32_t* s, int tid, int T, int logd) {
+template <int K, bool WL, int LV = 3>
+__device__ __forceinline__ void pass_store(const uint32_t (&v)[1 << LV], uint32_t* s, int tid, int T, int logd) {
 #pragma unroll
-    for (int m = 0; m < (8 >> K); ++m) {
-        const int tb = pass_thread_base<K, WL>(tid, T, m, logd);
+    for (int m = 0; m < ((1 << LV) >> K); ++m) {
+        const int tb = pass_thread_base<K, WL, LV>(tid, T, m, logd);
 #pragma unroll
         for (int l = 0; l < (1 << K); ++l) s[tb ^ swz(l << logd)] = v[(m << K) + l];
     }
 }
 
-template <int K, bool WL>
-__device__ __forceinline__ void pass_load(uint32_t (&v)[8], const uint32_t* s, int tid, int T, int logd) {
+template <int K, bool WL, int LV = 3>
+__device__ __forceinline__ void pass_load(uint32_t (&v)[1 << LV], const uint32_t* s, int tid, int T, int logd) {
 #pragma unroll
-    for (int m = 0; m < (8 >> K); ++m) {
-        const int tb = pass_thread_base<K, WL>(tid, T, m, logd);
+    for (int m = 0; m < ((1 << LV) >> K); ++m) {
+        const int tb = pass_thread_base<K, WL, LV>(tid, T, m, logd);
 #pragma unroll
         for (int l = 0; l < (1 << K); ++l) v[(m << K) + l] = s[tb ^ swz(l << logd)];
     }
 }
 
-template <int K, bool WL>
-__device__ __forceinline__ void pass_forward(uint32_t (&va)[8], uint32_t (&vb)[8], int tid, int T, int s0, int logd,
-                                             const uint2* tw, uint32_t p, uint32_t two_p) {
+template <int K, bool WL, int LV = 3>
+__device__ __forceinline__ void pass_forward(uint32_t (&va)[1 << LV], uint32_t (&vb)[1 << LV], int tid, int T, int s0,
+                                             int logd, const uint2* tw, uint32_t p, uint32_t two_p) {
 #pragma unroll
-    for (int m = 0; m < (8 >> K); ++m) {
-        const int blk = pass_gid<K, WL>(tid, T, m) >> logd;
+    for (int m = 0; m < ((1 << LV) >> K); ++m) {
+        const int blk = pass_gid<K, WL, LV>(tid, T, m) >> logd;
 #pragma unroll
         for (int u = 0; u < K; ++u) {
             const int h = 1 << (K - 1 - u);
@@ -185,12 +186,12 @@ __device__ __forceinline__ void pass_forward(uint32_t (&va)[8], uint32_t (&vb)[8
     }
 }
 
-template <int K, bool WL>
-__device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, int s0, int logd, const uint2* tw,
+template <int K, bool WL, int LV = 3>
+__device__ __forceinline__ void pass_inverse(uint32_t (&v)[1 << LV], int tid, int T, int s0, int logd, const uint2* tw,
                                              uint32_t p, uint32_t two_p) {
 #pragma unroll
-    for (int m = 0; m < (8 >> K); ++m) {
-        const int blk = pass_gid<K, WL>(tid, T, m) >> logd;
+    for (int m = 0; m < ((1 << LV) >> K); ++m) {
+        const int blk = pass_gid<K, WL, LV>(tid, T, m) >> logd;
 #pragma unroll
         for (int u = K - 1; u >= 0; --u) {
             const int h = 1 << (K - 1 - u);
@@ -204,7 +205,7 @@ __device__ __forceinline__ void pass_inverse(uint32_t (&v)[8], int tid, int T, i
     }
 }
 
-// The barrier after an exchange store: only the warp when both layouts keep it in its 256 words.
+// The barrier after an exchange store: only the warp when both layouts keep it in its 32V words.
 __device__ __forceinline__ void exchange_sync(bool warp_local) {
     if (warp_local)
         __syncwarp();
@@ -214,8 +215,8 @@ __device__ __forceinline__ void exchange_sync(bool warp_local) {
 
 // The forward row stages of a and b, the pointwise product and the inverse row
 // stages of one row, starting from the values a thread holds for the first pass
-// (pass_index<KP> with s0 = 0) and ending with the product in the same places.
-// sa, sb: 2C words of exchange space; stf, sti: the row's twiddles.
+// (pass_index<KP, false, LV> with s0 = 0) and ending with the product in the
+// same places.  sa, sb: 2C words of exchange space; stf, sti: the row's twiddles.
 // Every exchange stores a thread's values back to the very words that thread
 // loaded in the pass (so no barrier is needed before the store), then meets the
 // others before the next pass loads its own layout.  after_last_load() runs on
@@ -225,56 +226,58 @@ struct NoHook {
     __device__ void operator()() const {}
 };
 
-template <int LOGC, int KP, class Hook = NoHook>
-__device__ __forceinline__ void row_transform(uint32_t (&va)[8], uint32_t (&vb)[8], uint32_t* sa, uint32_t* sb,
-                                              const uint2* stf, const uint2* sti, int tid, const PrimeConst& pc,
-                                              Hook after_last_load = Hook{}) {
+template <int LOGC, int KP, class Hook = NoHook, int LV = 3>
+__device__ __forceinline__ void row_transform(uint32_t (&va)[1 << LV], uint32_t (&vb)[1 << LV], uint32_t* sa,
+                                              uint32_t* sb, const uint2* stf, const uint2* sti, int tid,
+                                              const PrimeConst& pc, Hook after_last_load = Hook{}) {
     constexpr int C = 1 << LOGC;
-    constexpr int T = C / 8;
+    constexpr int T = C >> LV;
     constexpr int NP = LOGC / KP;   // full passes
     constexpr int REM = LOGC % KP;  // stages of the closing pass
-    constexpr bool WL = KP == 3 && T >= 32;
+    constexpr bool WL = KP == LV && T >= 32;
     constexpr int KR = REM > 0 ? REM : KP;  // closing pass radix (unused when REM = 0)
+    static_assert(KP <= LV, "a pass holds at most V values per group");
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
         const int s0 = KP * q, logd = LOGC - s0 - KP;
         if (q > 0) {
-            pass_load<KP, WL>(va, sa, tid, T, logd);
-            pass_load<KP, WL>(vb, sb, tid, T, logd);
+            pass_load<KP, WL, LV>(va, sa, tid, T, logd);
+            pass_load<KP, WL, LV>(vb, sb, tid, T, logd);
         }
-        pass_forward<KP, WL>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
+        pass_forward<KP, WL, LV>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
         if (q + 1 < NP || REM) {
-            pass_store<KP, WL>(va, sa, tid, T, logd);
-            pass_store<KP, WL>(vb, sb, tid, T, logd);
-            const bool next_local = q + 1 < NP ? pass_warp_local<KP, WL>(logd - KP) : pass_warp_local<KR, WL>(0);
-            exchange_sync(pass_warp_local<KP, WL>(logd) && next_local);
+            pass_store<KP, WL, LV>(va, sa, tid, T, logd);
+            pass_store<KP, WL, LV>(vb, sb, tid, T, logd);
+            const bool next_local =
+                q + 1 < NP ? pass_warp_local<KP, WL, LV>(logd - KP) : pass_warp_local<KR, WL, LV>(0);
+            exchange_sync(pass_warp_local<KP, WL, LV>(logd) && next_local);
         }
     }
     if constexpr (REM > 0) {
         const int s0 = KP * NP, logd = 0;
-        pass_load<REM, WL>(va, sa, tid, T, logd);
-        pass_load<REM, WL>(vb, sb, tid, T, logd);
-        pass_forward<REM, WL>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
+        pass_load<REM, WL, LV>(va, sa, tid, T, logd);
+        pass_load<REM, WL, LV>(vb, sb, tid, T, logd);
+        pass_forward<REM, WL, LV>(va, vb, tid, T, s0, logd, stf, pc.p, pc.two_p);
     }
     // pointwise product in Montgomery form (a factor 2^-32 the CRT scale removes), in [0, 2p)
 #pragma unroll
-    for (int l = 0; l < 8; ++l)
+    for (int l = 0; l < (1 << LV); ++l)
         va[l] = mont_mul(csub(va[l], pc.two_p), csub(vb[l], pc.two_p), pc.p, pc.pinv);
     if constexpr (REM > 0) {
         const int s0 = KP * NP, logd = 0;
-        pass_inverse<REM, WL>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
-        pass_store<REM, WL>(va, sa, tid, T, logd);
-        exchange_sync(pass_warp_local<REM, WL>(0) && pass_warp_local<KP, WL>(LOGC - KP * NP));
+        pass_inverse<REM, WL, LV>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
+        pass_store<REM, WL, LV>(va, sa, tid, T, logd);
+        exchange_sync(pass_warp_local<REM, WL, LV>(0) && pass_warp_local<KP, WL, LV>(LOGC - KP * NP));
     }
 #pragma unroll
     for (int q = NP - 1; q >= 0; --q) {
         const int s0 = KP * q, logd = LOGC - s0 - KP;
-        if (q + 1 < NP || REM) pass_load<KP, WL>(va, sa, tid, T, logd);
+        if (q + 1 < NP || REM) pass_load<KP, WL, LV>(va, sa, tid, T, logd);
         if (q == 0) after_last_load();
-        pass_inverse<KP, WL>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
+        pass_inverse<KP, WL, LV>(va, tid, T, s0, logd, sti, pc.p, pc.two_p);
         if (q > 0) {
-            pass_store<KP, WL>(va, sa, tid, T, logd);
-            exchange_sync(pass_warp_local<KP, WL>(logd) && pass_warp_local<KP, WL>(logd + KP));
+            pass_store<KP, WL, LV>(va, sa, tid, T, logd);
+            exchange_sync(pass_warp_local<KP, WL, LV>(logd) && pass_warp_local<KP, WL, LV>(logd + KP));
         }
     }
 }

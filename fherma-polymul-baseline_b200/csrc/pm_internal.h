@@ -65,7 +65,7 @@ struct PipelineSlot {
 
 // Launch shapes the autotuner chooses per plan (defaults apply until it runs).
 struct Tuning {
-    int row_radix_log = 3;   // K2 register-pass radix: 2 (radix-4) or 3 (radix-8)
+    int row_radix_log = 4;   // K2 register-pass radix: 2, 3 or 4 (radix 4, 8, 16; 16 in the persistent kernel)
     int conv_ctas_per_sm = 3;  // K1T persistent CTAs per SM (three fit its 128 registers a thread)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
     bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)

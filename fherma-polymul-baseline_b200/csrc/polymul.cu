@@ -440,27 +440,33 @@ void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStr
             const int64_t total = items * bt.count;
             const int ctas = int(std::min<int64_t>(total, int64_t(s.sms) * k2p_min_blocks(LOGC)));
             const PlanRowWork w{work, bt.ws_bstride, int(s.n), int(s.logR), int(s.logC), int(s.P), int(bt.count)};
-            k2p_rows<LOGC, KP, PlanRowWork><<<ctas, T, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_fwd,
-                                                                   s.basis->d_tw_inv, int(s.logR), s.d_err);
+            k2p_rows<LOGC, KP, PlanRowWork><<<ctas, k2p_threads(LOGC, KP), smem, st>>>(
+                w, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.logR), s.d_err);
             return;
         }
     }
-    int rows = T >= 128 ? 1 : 128 / T;
-    const int R = 1 << s.logR;
-    if (rows > R) rows = R;
-    const size_t smem = size_t(rows) * 24 * C;  // 2C uint2 twiddles + 2C words of data per row
-    if (smem > 48 * 1024)
-        cuda_check(cudaFuncSetAttribute(k2_rows<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                   "raise K2 shared memory");
-    dim3 grid(R / rows, s.P, bt.count), block(rows * T);
-    k2_rows<LOGC, KP><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.n),
-                                             int(s.logR), int(s.P), bt.ws_bstride);
+    if constexpr (KP == 4) {  // radix-16 passes exist in the persistent kernel only
+        launch_k2_fixed<LOGC, 3>(s, work, bt, st);
+    } else {
+        int rows = T >= 128 ? 1 : 128 / T;
+        const int R = 1 << s.logR;
+        if (rows > R) rows = R;
+        const size_t smem = size_t(rows) * 24 * C;  // 2C uint2 twiddles + 2C words of data per row
+        if (smem > 48 * 1024)
+            cuda_check(cudaFuncSetAttribute(k2_rows<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                       "raise K2 shared memory");
+        dim3 grid(R / rows, s.P, bt.count), block(rows * T);
+        k2_rows<LOGC, KP><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
+                                                     int(s.n), int(s.logR), int(s.P), bt.ws_bstride);
+    }
 }
 
 template <int LOGC>
 void launch_k2_radix(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t st) {
     if (s.tune.row_radix_log == 2)
         launch_k2_fixed<LOGC, 2>(s, work, bt, st);
+    else if (LOGC >= 10 && s.tune.row_radix_log == 4)
+        launch_k2_fixed<LOGC, LOGC >= 10 ? 4 : 3>(s, work, bt, st);
     else
         launch_k2_fixed<LOGC, 3>(s, work, bt, st);
 }

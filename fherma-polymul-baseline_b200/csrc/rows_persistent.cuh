@@ -17,9 +17,12 @@
 //     the next item's rows are requested into it, landing while this item's
 //     last stages run and its product row is stored.
 // One data buffer instead of two keeps a CTA at 48 KB (C = 2048), so four CTAs
-// (with at most 64 registers a thread) share an SM; at C = 4096, 96 KB and two.  One row per CTA
-// (T = C/8 threads), C >= 1024.  Bulk copies need 16-byte aligned rows: the
-// host launches this kernel only on 16-byte aligned workspaces.
+// share an SM; at C = 4096, 96 KB and two.  One row per CTA, C >= 1024, with
+// T = C/16 threads of 16 values (radix-16 passes, the default: two exchanges
+// per direction instead of three, up to 128 registers a thread) or T = C/8
+// threads of 8 values (radix 4 or 8, at most 64 registers).  Bulk copies need
+// 16-byte aligned rows: the host launches this kernel only on 16-byte aligned
+// workspaces.
 //
 // Dynamic shared memory: C uint2 forward and C uint2 inverse twiddles, one data
 // buffer of 2C words, two mbarriers (data, twiddles): 24C + 16 B.
@@ -52,13 +55,17 @@ struct PlanRowWork {
 };
 
 constexpr int k2p_min_blocks(int logc) { return logc >= 12 ? 2 : (logc >= 11 ? 4 : 8); }
+// values a thread: 16 for radix-16 passes (KP = 4), else 8
+constexpr int k2p_lv(int kp) { return kp == 4 ? 4 : 3; }
+constexpr int k2p_threads(int logc, int kp) { return (1 << logc) >> k2p_lv(kp); }
 constexpr size_t k2p_smem_bytes(int logc) { return (size_t(24) << logc) + 2 * sizeof(uint64_t); }
 
 template <int LOGC, int KP, class Work>
-__global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
+__global__ void __launch_bounds__(k2p_threads(LOGC, KP), k2p_min_blocks(LOGC))
     k2p_rows(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs, const uint2* __restrict__ tw_fwd,
              const uint2* __restrict__ tw_inv, int logR, uint32_t* __restrict__ err) {
-    constexpr int C = 1 << LOGC, T = C / 8;
+    constexpr int LV = k2p_lv(KP), V = 1 << LV;
+    constexpr int C = 1 << LOGC, T = C >> LV;
     constexpr int logd0 = LOGC - KP;  // first pass: s0 = 0
     static_assert(LOGC >= 10, "one row per CTA needs C >= 1024");
     extern __shared__ __align__(16) uint2 smem2[];
@@ -130,12 +137,12 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
 
         uint32_t* sa = sd;
         uint32_t* sb = sa + C;
-        uint32_t va[8], vb[8];
+        uint32_t va[V], vb[V];
 #pragma unroll
-        for (int m = 0; m < (8 >> KP); ++m)
+        for (int m = 0; m < (V >> KP); ++m)
 #pragma unroll
             for (int l = 0; l < (1 << KP); ++l) {
-                const int idx = pass_index<KP>(tid, T, m, l, logd0);
+                const int idx = pass_index<KP, false, LV>(tid, T, m, l, logd0);
                 va[(m << KP) + l] = sa[idx];
                 vb[(m << KP) + l] = sb[idx];
             }
@@ -143,19 +150,20 @@ __global__ void __launch_bounds__((1 << LOGC) / 8, k2p_min_blocks(LOGC))
         // has its values before any exchange store lands in this buffer
         __syncthreads();
         // once every thread holds the last pass's values, the buffer takes the next item's rows
-        row_transform<LOGC, KP>(va, vb, sa, sb, stf, sti, tid, pc, [&]() {
+        auto hook = [&]() {
             tc::fence_smem_async();
             __syncthreads();
             if (k + 1 < end) {
                 if (tid == 0) issue_rows(k + 1);
                 pending |= 1u;
             }
-        });
+        };
+        row_transform<LOGC, KP, decltype(hook), LV>(va, vb, sa, sb, stf, sti, tid, pc, hook);
         uint32_t* ga = it.a;
 #pragma unroll
-        for (int m = 0; m < (8 >> KP); ++m)
+        for (int m = 0; m < (V >> KP); ++m)
 #pragma unroll
-            for (int l = 0; l < (1 << KP); ++l) ga[pass_index<KP>(tid, T, m, l, logd0)] = va[(m << KP) + l];
+            for (int l = 0; l < (1 << KP); ++l) ga[pass_index<KP, false, LV>(tid, T, m, l, logd0)] = va[(m << KP) + l];
         // this thread's shared-memory writes are ordered before the next bulk copy into this buffer
         tc::fence_smem_async();
         if (__syncthreads_or(!ok)) break;

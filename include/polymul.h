@@ -80,7 +80,8 @@ int pm_plan_get_info(const pm_plan* plan, pm_plan_info* info);
 
 /* Launch shapes of a plan (see pm_plan_autotune). */
 typedef struct {
-    uint32_t row_radix;         /* radix of the row NTT register passes: 4 or 8 */
+    uint32_t row_radix;         /* radix of the row NTT register passes: 4, 8 or 16 (16: rows of >= 1024
+                                   values in the persistent kernel; other rows then use 8) */
     uint32_t conv_ctas_per_sm;  /* persistent CTAs of the tensor conversion per SM, 1..8 */
     uint32_t crt_ctas_per_sm;   /* persistent CTAs of the tensor CRT per SM, 1..4 */
     uint32_t group;             /* products per launch group in batched calls (0: up to ~1 GB of residues, <= 64) */

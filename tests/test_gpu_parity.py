@@ -215,7 +215,8 @@ def test_tunings_do_not_change_results(cuda, path, n):
     ref = None
     with make_plan(path, n, q, 14) as p:
         shapes = [(8, 4, 2, 0, 1), (4, 4, 2, 0, 1), (8, 2, 1, 1, 1), (4, 3, 1, 2, 1), (8, 4, 2, 5, 1),
-                  (8, 4, 2, 0, 0), (4, 4, 2, 3, 0), (8, 4, 2, 3, 1)]
+                  (8, 4, 2, 0, 0), (4, 4, 2, 3, 0), (8, 4, 2, 3, 1), (16, 3, 2, 0, 1), (16, 3, 2, 3, 1),
+                  (16, 3, 2, 2, 0)]
         for radix, conv, crt, group, persistent in shapes:
             p.set_tuning(radix, conv, crt, group, persistent)
             c = torch.zeros_like(a)
@@ -225,7 +226,7 @@ def test_tunings_do_not_change_results(cuda, path, n):
                 ref = c.clone()
             assert torch.equal(c, ref), (radix, conv, crt, group, persistent)
         chosen = p.autotune()
-        assert chosen["row_radix"] in (4, 8) and chosen["us_per_product"] > 0
+        assert chosen["row_radix"] in (4, 8, 16) and chosen["us_per_product"] > 0
         c = torch.zeros_like(a)
         p.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), count)
         torch.cuda.synchronize()
