@@ -346,8 +346,9 @@ struct BatchCore {
                 std::stable_sort(items.begin(), items.end(), [](const uint4& x, const uint4& y) {
                     return x.y != y.y ? x.y < y.y : x.z < y.z;
                 });
-            // the radix the autotuner picked for plans of this row size, radix-8 by default
-            int radix_log = 3;
+            // the radix the autotuner picked for plans of this row size; by default radix 16
+            // for the persistent kernel's rows (C >= 1024), radix 8 below
+            int radix_log = logC >= 10 ? 4 : 3;
             for (auto& p : plans)
                 if (int(p->logC) == logC && p->tune.tuned) radix_log = p->tune.row_radix_log;
             row_classes.push_back(RowClass{logC, radix_log, rows_per_item[logC], int(items.size()), row_items.size()});
@@ -440,10 +441,12 @@ struct BatchCore {
             undo();
             capture();
         };
-        for (auto& rc : row_classes) {
-            const int old = rc.radix_log;
-            attempt([&] { rc.radix_log = old == 3 ? 2 : 3; }, [&] { rc.radix_log = old; });
-        }
+        for (auto& rc : row_classes)
+            for (int k : {2, 3, 4}) {
+                const int cur = rc.radix_log;
+                if (k == cur || (k == 4 && rc.logC < 10)) continue;  // radix 16: persistent kernel rows only
+                attempt([&] { rc.radix_log = k; }, [&] { rc.radix_log = cur; });
+            }
         for (int k : {2, 3, 4}) {
             const int old = conv_ctas_per_sm;
             if (k == old) continue;
