@@ -152,6 +152,7 @@ void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
     const int items = pgs * int(count) * 2 * (C / Gc);
     int ctas = sm_count() * s.tune.conv_ctas_per_sm;
     if (ctas > items) ctas = items;
+    if (ctas >= pgs) ctas -= ctas % pgs;  // equal numbers of CTAs per prime group (PlanConvWork::range)
     if (ctas < 1) ctas = 1;
     const size_t smem = k1t_smem_bytes();
     cuda_check(cudaFuncSetAttribute(k1t_convert<LOGR, PlanConvWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,

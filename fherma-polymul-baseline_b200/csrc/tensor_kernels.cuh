@@ -93,6 +93,22 @@ struct PlanConvWork {
     __device__ ConvTarget target(int z, int poly) const {
         return ConvTarget{poly ? &map_b : &map_a, z, work + z * ws_bstride, n, logC, P};
     }
+    // CTA b of `grid` (a multiple of pgs): prime group b / m, m = grid / pgs, and the
+    // (b % m)-th of m equal runs of that group's tiles.  The CTAs of different prime groups
+    // with the same run read the same coefficient tiles at about the same time, so three of
+    // every four TMA loads of a tile hit L2 instead of streaming the inputs once per group.
+    __device__ int2 range(int b, int grid) const {
+        const int per_pg = count << (lg() + 1);
+        const int m = grid / pgs;
+        if (m == 0) {  // fewer CTAs than prime groups: contiguous runs of everything
+            const int all = total(), chunk = (all + grid - 1) / grid;
+            return make_int2(min(all, b * chunk), min(all, (b + 1) * chunk));
+        }
+        const int pg = b / m, j = b - pg * m;
+        if (pg >= pgs) return make_int2(0, 0);
+        const int chunk = (per_pg + m - 1) / m;
+        return make_int2(pg * per_pg + min(j * chunk, per_pg), pg * per_pg + min((j + 1) * chunk, per_pg));
+    }
 };
 
 struct TableConvWork {
@@ -109,6 +125,10 @@ struct TableConvWork {
     __device__ ConvTarget target(int z, int poly) const {
         const BatchProduct& d = prod[z];
         return ConvTarget{maps + 3 * z + poly, 0, work + d.ws_off, d.n, d.logC, d.P};
+    }
+    __device__ int2 range(int b, int grid) const {  // contiguous runs of the table
+        const int chunk = (nitems + grid - 1) / grid;
+        return make_int2(min(nitems, b * chunk), min(nitems, (b + 1) * chunk));
     }
 };
 
@@ -198,10 +218,8 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
     __shared__ uint2 spm[tc::kConvGroup];  // the group's primes and floor(2^48 / p)
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int total = w.total();
-    const int chunk = (total + int(gridDim.x) - 1) / int(gridDim.x);
-    const int begin = int(blockIdx.x) * chunk;
-    const int end = min(total, begin + chunk);
+    const int2 range = w.range(int(blockIdx.x), int(gridDim.x));
+    const int begin = range.x, end = range.y;
 
     for (int k = tid; k < 2048; k += tc::kConvThreads) reinterpret_cast<uint4*>(sA)[k] = make_uint4(0, 0, 0, 0);
     if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
