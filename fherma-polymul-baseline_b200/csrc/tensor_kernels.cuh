@@ -565,8 +565,9 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int J = 16 * q + 4 * u;  // first byte column of this 32-bit word
-                const uint64_t s = uint64_t(d[4 * u]) + (uint64_t(d[4 * u + 1]) << 8) +
-                                   (uint64_t(d[4 * u + 2]) << 16) + (uint64_t(d[4 * u + 3]) << 24);
+                // column sums d <= 256 * 255^2: d0 + 2^8 d1 and d2 + 2^8 d3 are below 2^32
+                const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8), hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
+                const uint64_t s = uint64_t(lo) + (uint64_t(hi) << 16);
                 if (J < NV) {
                     const uint64_t x = s + carry;
                     acc[J / 4] = uint32_t(x);
