@@ -63,10 +63,10 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
         }
     }
     if (reps == 0) reps = 3;
-    // a batch big enough for the largest group tried, capped at ~2 GB of buffers
+    // a batch big enough for the largest group tried, capped at ~4 GB of buffers
     const size_t per = 3 * s.io_bytes + s.workspace_bytes;
-    uint32_t count = uint32_t((size_t(2048) << 20) / per);
-    count = count < 1 ? 1 : (count > 64 ? 64 : count);
+    uint32_t count = uint32_t((size_t(4096) << 20) / per);
+    count = count < 1 ? 1 : (count > kMaxDefaultGroup ? kMaxDefaultGroup : count);
     Scratch sc;
     cuda_check(cudaStreamCreateWithFlags(&sc.st, cudaStreamNonBlocking), "autotune stream");
     cuda_check(cudaEventCreate(&sc.e0), "autotune event");
@@ -132,7 +132,7 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
             if (k != best.crt_ctas_per_sm) consider(t);
         }
     }
-    for (uint32_t g : {4u, 8u, 16u, 32u, 64u}) {
+    for (uint32_t g : {4u, 8u, 16u, 32u, 64u, 128u}) {
         if (g > count) break;
         Tuning t = best;
         t.group = g;
@@ -179,7 +179,7 @@ extern "C" int pm_plan_set_tuning(pm_plan* plan, const pm_tuning* t) {
         return pm::fail(PM_ERR_INVALID, "row_radix must be 4, 8 or 16");
     if (t->conv_ctas_per_sm < 1 || t->conv_ctas_per_sm > 8 || t->crt_ctas_per_sm < 1 || t->crt_ctas_per_sm > 4)
         return pm::fail(PM_ERR_INVALID, "CTAs per SM out of range");
-    if (t->group > 64) return pm::fail(PM_ERR_INVALID, "group above 64");
+    if (t->group > pm::kMaxGroup) return pm::fail(PM_ERR_INVALID, "group above 256");
     if (t->row_persistent > 1) return pm::fail(PM_ERR_INVALID, "row_persistent must be 0 or 1");
     pm::Tuning& u = plan->core.tune;
     u.row_radix_log = t->row_radix == 4 ? 2 : (t->row_radix == 8 ? 3 : 4);

@@ -84,7 +84,8 @@ typedef struct {
                                    values in the persistent kernel; other rows then use 8) */
     uint32_t conv_ctas_per_sm;  /* persistent CTAs of the tensor conversion per SM, 1..8 */
     uint32_t crt_ctas_per_sm;   /* persistent CTAs of the tensor CRT per SM, 1..4 */
-    uint32_t group;             /* products per launch group in batched calls (0: up to ~1 GB of residues, <= 64) */
+    uint32_t group;             /* products per launch group in batched calls (0: up to ~2 GB of residues and
+                                   128 products; at most 256) */
     uint32_t row_persistent;    /* 1: rows of >= 1024 values by the persistent kernel that stages a row's
                                    twiddles once per group and prefetches rows; 0: one CTA per row */
     double us_per_product;      /* device time the autotuner measured (-1: taken from its cache) */
@@ -120,8 +121,8 @@ int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c
 /*
  * A batch of `count` products of one plan, stored back to back: a, b, c are
  * device arrays [count][n][coef_limbs].  The library runs them in launch
- * groups (one launch per pass covers a group; by default up to ~1 GB of residue
- * planes, 64 products at n = 32768, or the autotuner's choice).  workspace: a
+ * groups (one launch per pass covers a group; by default up to ~2 GB of residue
+ * planes, 128 products at n = 32768, or the autotuner's choice).  workspace: a
  * device buffer of workspace_bytes (at least one product's worth; a smaller
  * buffer than a group needs shrinks the group, see pm_batch_workspace_size), or
  * NULL to use a plan-owned buffer that the first call allocates.  Asynchronous
