@@ -70,7 +70,7 @@ constexpr uint32_t kMaxGroup = 256;
 // Launch shapes the autotuner chooses per plan (defaults apply until it runs).
 struct Tuning {
     int row_radix_log = 4;   // K2 register-pass radix: 2, 3 or 4 (radix 4, 8, 16; 16 in the persistent kernel)
-    int conv_ctas_per_sm = 3;  // K1T persistent CTAs per SM (three fit its 128 registers a thread)
+    int conv_ctas_per_sm = 3;  // K1T persistent CTAs per SM (up to four fit; three measured fastest)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
     bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)
     uint32_t group = 0;        // products per launch group in batches (0: up to ~2 GB of residues, <= 128)

@@ -185,10 +185,10 @@ struct TableCrtWork {
 // N=64, K=32) into that accumulator, commit; once the MMA is complete its A tile
 // takes the TMA of the item two ahead.
 // Workers: wait for the item's MMA, tcgen05.ld -> two 32-bit partial sums ->
-// lazy Barrett (the group's primes and factors held in registers: 128 registers
-// a thread at R = 16, three CTAs per SM) -> padded transpose, release the
-// accumulator (mbarrier arrival), then 4 forward column stages in registers ->
-// residue planes.  Only the workers meet at (named) barriers, so the producer's
+// lazy Barrett (the group's primes and factors held in registers, the column
+// twiddles in shared memory: 96 registers a thread, so four CTAs fit per SM) ->
+// padded transpose, release the accumulator (mbarrier arrival), then 4 forward
+// column stages in registers -> residue planes.  Only the workers meet at (named) barriers, so the producer's
 // waits never hold them.
 // Barriers: tma_full[2], mma_full[2], tmem_empty[2] (128 arrivals), b_full.
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB, B 8 KB, transpose
@@ -201,7 +201,7 @@ constexpr int kConvThreads = 160;
 }
 
 template <int LOGR, class Work>
-__global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_constant__ Work w,
+__global__ void __launch_bounds__(tc::kConvThreads, 4) k1t_convert(const __grid_constant__ Work w,
                                                                 const PrimeConst* __restrict__ pcs,
                                                                 const uint8_t* __restrict__ conv_w,
                                                                 const uint2* __restrict__ tw_fwd,
@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
     __shared__ uint32_t tmem_base;
     __shared__ volatile uint32_t s_abort;
     __shared__ uint2 spm[tc::kConvGroup];  // the group's primes and floor(2^48 / p)
+    __shared__ uint2 stw[tc::kConvGroup][R > 1 ? R - 1 : 1];  // the group's forward column twiddles
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int2 range = w.range(int(blockIdx.x), int(gridDim.x));
@@ -313,7 +314,6 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
         const uint32_t taddr = tbase + (uint32_t(32 * warp) << 16);
         // column-stage role: prime j of the group, column c of the tile
         const int cj = tid / 8, cc = tid % 8;
-        uint2 twr[R > 1 ? R - 1 : 1];
         uint2 rpm[tc::kConvGroup];  // the group's primes and floor(2^48 / p)
         PrimeConst cpc{};
         int cur_pg = -1;
@@ -330,8 +330,10 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
                     spm[tid] = make_uint2(g.p, g.mu >> 13);  // floor(floor(2^61 / p) / 2^13)
                 }
                 const int ci = it.pg * tc::kConvGroup + cj;
-#pragma unroll
-                for (int q = 1; q < R; ++q) twr[q - 1] = __ldg(tw_fwd + size_t(ci) * kNMax + q);
+                constexpr int RT = R > 1 ? R - 1 : 1;
+                if (R > 1)
+                    for (int q = tid; q < tc::kConvGroup * RT; q += 128)
+                        stw[q / RT][q % RT] = __ldg(tw_fwd + size_t(it.pg * tc::kConvGroup + q / RT) * kNMax + 1 + q % RT);
                 cpc = pcs[ci];
                 cur_pg = it.pg;
                 tc::bar_sync(1, 128);
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(tc::kConvThreads) k1t_convert(const __grid_con
 #pragma unroll
                     for (int r = 0; r < R; ++r)
                         if (!(r & h))
-                            ct_bfly(v[r], v[r + h], twr[(1 << s) + (r >> (LOGR - s)) - 1], cpc.p, cpc.two_p);
+                            ct_bfly(v[r], v[r + h], stw[cj][(1 << s) + (r >> (LOGR - s)) - 1], cpc.p, cpc.two_p);
                 }
                 uint32_t* dst = t.res + (size_t(it.poly) * t.P + ci) * t.n + size_t(it.cg) * Gc + cc;
                 const size_t row = size_t(1) << t.logC;
