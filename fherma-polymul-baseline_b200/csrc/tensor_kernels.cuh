@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         const int pairs = t.P * Gc;
         for (int pr = tid; pr < pairs; pr += tc::kCrtThreads) {
             const int i = pr / Gc, c = pr - i * Gc;
-            const PrimeConst pc = pcs[i];
+            const uint32_t p = __ldg(&pcs[i].p), two_p = 2 * p;
             uint32_t v[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) v[r] = sR[(r * t.P + i) * Gc + c];
@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
                 const int h = R >> (s + 1);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (!(r & h)) gs_bfly(v[r], v[r + h], tw[(1 << s) + (r >> (LOGR - s))], pc.p, pc.two_p);
+                    if (!(r & h)) gs_bfly(v[r], v[r + h], tw[(1 << s) + (r >> (LOGR - s))], p, two_p);
             }
             // last stage (one twiddle per prime) with the CRT scale s_i folded in:
             // x' = s_i (x + y), y' = s_i w (x - y); digits t_i in [0, 2p) (an extra p_i
@@ -523,11 +523,11 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
 #pragma unroll
                 for (int r = 0; r < R / 2; ++r) {
                     const uint32_t x = v[r], y = v[r + R / 2];
-                    v[r] = shoup_mul(x + y, sc, pc.p);
-                    v[r + R / 2] = shoup_mul(x - y + pc.two_p, sw, pc.p);
+                    v[r] = shoup_mul(x + y, sc, p);
+                    v[r + R / 2] = shoup_mul(x - y + two_p, sw, p);
                 }
             } else {
-                v[0] = shoup_mul(v[0], sc, pc.p);
+                v[0] = shoup_mul(v[0], sc, p);
             }
             const uint32_t ka = uint32_t(i) >> 5, kb = (4u * i) & 127u;
 #pragma unroll
