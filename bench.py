@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--bits", type=int, default=868)
     ap.add_argument("--batch", type=int, default=512, help="independent products per step")
     ap.add_argument("--e2e-batch", type=int, default=0,
-                    help="products per step of the end-to-end (host buffer) measurement; 0: the same as --batch")
+                    help="products per step of the end-to-end (host buffer) measurement; 0: the same as "
+                         "--batch on one GPU, 64 per rank on several")
     ap.add_argument("--path", default="tensor", choices=["tensor", "simt"],
                     help="tensor: tcgen05 INT8 conversion/CRT (default); simt: the plain CUDA-core method")
     ap.add_argument("--seed", type=int, default=20261203)
@@ -686,7 +687,8 @@ def run_ours(args):
     plain = run_plain(args, torch, plan, A, Bv, Cv, stream, value / world)
 
     # end to end through the C ABI host-buffer call, pinned host memory
-    E = min(args.e2e_batch or B, B)
+    # the whole batch on one GPU; 64 products a rank when several ranks share the host's pinned memory
+    E = min(args.e2e_batch or (B if world == 1 else 64), B)
     ha = torch.empty((E, n, limbs), dtype=torch.int64, pin_memory=True)
     hb = torch.empty_like(ha, pin_memory=True)
     hc = torch.empty_like(ha, pin_memory=True)
