@@ -236,6 +236,35 @@ def test_tunings_do_not_change_results(cuda, path, n):
         assert (ref[k].cpu().numpy().view(np.uint64) == oracle.rns_multiply(ak, bk, q)).all()
 
 
+def test_tuning_limits_and_large_default_groups(cuda):
+    """pm_plan_set_tuning refuses shapes outside its documented ranges; a batch of more
+    products than the default launch group (128) runs in a full group and a tail, with the
+    same bits as groups of one and the oracle's."""
+    torch = cuda
+    rng = np.random.default_rng(77)
+    q = random_q(rng, 868)
+    n, count = 1024, 131
+    with make_plan("tensor", n, q, 14) as p:
+        for bad in [dict(row_radix=32), dict(group=257), dict(conv_ctas_per_sm=0), dict(crt_ctas_per_sm=5),
+                    dict(row_persistent=2)]:
+            with pytest.raises(polymul.PolymulError):
+                p.set_tuning(**bad)
+        p.set_tuning(group=256)
+        a = torch.from_numpy(np.stack([uniform_below(rng, q, n, 14) for _ in range(count)]).view(np.int64)).cuda()
+        b = torch.from_numpy(np.stack([uniform_below(rng, q, n, 14) for _ in range(count)]).view(np.int64)).cuda()
+        outs = []
+        for group in (0, 1):
+            p.set_tuning(group=group)
+            c = torch.zeros_like(a)
+            p.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), count)
+            torch.cuda.synchronize()
+            outs.append(c)
+        assert torch.equal(outs[0], outs[1])
+    for k in (0, 127, 128, count - 1):
+        ak, bk = a[k].cpu().numpy().view(np.uint64), b[k].cpu().numpy().view(np.uint64)
+        assert (outs[0][k].cpu().numpy().view(np.uint64) == oracle.rns_multiply(ak, bk, q)).all()
+
+
 def test_bad_device_pointers_are_refused(cuda, path):
     """Misaligned or pageable pointers are caught on the host, before any kernel runs."""
     torch = cuda
