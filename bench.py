@@ -9,15 +9,19 @@ One JSON line on rank 0 (contract of the driver):
   roofline   the dominant kernel's algorithmic bytes per launch / its mean
              device time (CUDA events on its launch stream, recorded by the
              library during the timed steps);
-  cpu_baseline  the CPU restatement of the reference method (oracle/, all host
-             threads) on a bounded sample of the same workload.
+  cpu_baseline  the reference's own rns kernels run by its CPU emulation
+             (oracle/_ref/rns_emulated, one product per host core at once) on a
+             bounded sample of the same workload; the C restatement of the
+             method (oracle/, all host threads) beside it.
 
 Multi-GPU is replicas only: the method has no exchange step between products,
 so each rank runs its own batch and value sums products over the max-over-
 ranks device time.
 
---impl reference times the reference's method on the host cores (the oracle
-port: the reference's own path needs cuPQC and a GPU) on the same workload.
+--impl reference times the reference's CPU path on the host cores: its own
+rns kernel bodies under its CPU emulation (its GPU path needs the closed cuPQC
+SDK), one single-threaded process per core, a step being one product at the
+same N and width (q = 2^868 - 11993087: the only form that backend takes).
 """
 import argparse
 import json
@@ -53,7 +57,8 @@ def parse():
     ap.add_argument("--path", default="tensor", choices=["tensor", "simt"],
                     help="tensor: tcgen05 INT8 conversion/CRT (default); simt: the plain CUDA-core method")
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-seconds", type=float, default=5.0,
+                    help="seconds of the C restatement's sample (0 skips every CPU baseline)")
     ap.add_argument("--serve-requests", type=int, default=10000,
                     help="requests in the serving stream (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=6000.0, help="Poisson arrival rate, requests/s")
@@ -137,10 +142,98 @@ def host_inputs(n, q, seed, count=1):
     return [(uniform_below(rng, q, n, limbs), uniform_below(rng, q, n, limbs)) for _ in range(count)]
 
 
+FHERMA_Q = (1 << 868) - 11993087  # the reference's point: its rns backend takes only q = 2^868 - c, c < 2^28
+
+
+def emulated_reference_sample(n, products, workers, seed):
+    """The reference's own rns kernels, CPU-emulated (oracle/_ref/rns_emulated): `products`
+    products at (n, 2^868 - 11993087) split over `workers` concurrent processes (the
+    emulation runs one host thread each).  Returns (products/s over the wall time of the
+    whole sample, wall seconds, per-case seconds, one (a, b, c) triple to check)."""
+    import tempfile
+
+    import numpy as np
+
+    from tests import reference_emulation as emu
+    from tests.helpers import uniform_below
+
+    rng = np.random.default_rng(seed)
+    pairs = [(uniform_below(rng, FHERMA_Q, n, 14), uniform_below(rng, FHERMA_Q, n, 14)) for _ in range(products)]
+    workers = max(1, min(workers, products))
+    parts = [pairs[w::workers] for w in range(workers)]
+    with tempfile.TemporaryDirectory() as tmp:
+        dirs = []
+        for w, part in enumerate(parts):
+            d = os.path.join(tmp, f"w{w}")
+            emu.write_point(d, n, FHERMA_Q, part)
+            dirs.append(d)
+        t0 = time.perf_counter()
+        procs = [emu.start(d) for d in dirs]
+        for p in procs:
+            _, err = p.communicate()
+            if p.returncode != 0:
+                raise RuntimeError(f"emulated reference failed: {err[-300:]}")
+        wall = time.perf_counter() - t0
+        secs = []
+        outs0 = None
+        for w, (d, part) in enumerate(zip(dirs, parts)):
+            outs, sec = emu.read_results(d, len(part), n)
+            secs += sec
+            if w == 0:
+                outs0 = outs[0]
+    a, b = parts[0][0]
+    return products / wall, wall, secs, (a, b, outs0)
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def run_reference(args):
+    """The reference's CPU path on the host cores: its own rns kernel bodies run by its CPU
+    emulation (oracle/_ref/rns_emulated, one host thread per process), one process per core;
+    a step is one product at the bench's N.  Falls back to the oracle's C restatement of the
+    method (threads over primes) when the emulated binary was not built."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
+    from tests import reference_emulation as emu
+
+    cores = host_cores()
+    base = {
+        "impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+    }
+    if emu.available():
+        import numpy as np
+
+        from oracle import oracle
+
+        # warm-up: the binary, libgmp and the page cache, on small rings
+        emulated_reference_sample(1024, max(1, min(args.warmup, cores)), cores, args.seed + 2)
+        value, wall, secs, (a, b, c) = emulated_reference_sample(args.ring, args.steps, cores, args.seed + 1)
+        if not (c == oracle.rns_multiply(a, b, FHERMA_Q)).all():
+            raise SystemExit("emulated reference disagrees with the oracle")
+        per = sorted(secs)
+        line = dict(base, value=value, ms_per_step=1000 * wall / args.steps)
+        line["config"] = {"workload": f"one negacyclic product per step, N={args.ring}, 868-bit q = 2^868 - 11993087 "
+                                      "(the reference's rns backend takes only q = 2^868 - c), coefficients uniform "
+                                      "in [0, q)", "n": args.ring, "q_bits": 868,
+                          "parallelism": f"{min(cores, args.steps)} concurrent single-threaded processes"}
+        line["cpu_baseline"] = {"value": value, "unit": UNIT, "cores": min(cores, args.steps), "kind": "reference",
+                                "sample": f"{args.steps} products at N={args.ring} through the reference's own rns "
+                                          "kernels (rns/solve.cu) run by its CPU emulation (tests/build_emulation.py "
+                                          "rewrite, GMP big integers), one process per core; "
+                                          f"{per[len(per) // 2]:.1f} s per product (median)",
+                                "seconds_per_product_median": per[len(per) // 2]}
+        line["e2e"] = {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        print(json.dumps(line), flush=True)
+        return
+
     threads = os.cpu_count() or 1
     q = seeded_q(args.seed, args.bits)
     (a, b), = host_inputs(args.ring, q, args.seed + 1)
@@ -153,19 +246,15 @@ def run_reference(args):
         oracle.rns_multiply(a, b, q, threads=threads)
     el = time.perf_counter() - t0
     value = args.steps / el
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"one negacyclic product per step, N={args.ring}, {args.bits}-bit seeded odd q, "
-                               "coefficients uniform in [0, q)", "n": args.ring, "q_bits": args.bits,
-                   "parallelism": "cpu threads"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} products at N={args.ring}; the reference's RNS method restated in C "
-                                   "(oracle/polymul_oracle.c), threads over primes; the reference's own path "
-                                   "needs cuPQC and a GPU"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    line = dict(base, value=value, ms_per_step=1000 * el / args.steps)
+    line["config"] = {"workload": f"one negacyclic product per step, N={args.ring}, {args.bits}-bit seeded odd q, "
+                                  "coefficients uniform in [0, q)", "n": args.ring, "q_bits": args.bits,
+                      "parallelism": "cpu threads"}
+    line["cpu_baseline"] = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": f"{args.steps} products at N={args.ring}; the reference's RNS method restated "
+                                      "in C (oracle/polymul_oracle.c), threads over primes (the emulated reference "
+                                      "binary was not built)"}
+    line["e2e"] = {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
 
 
@@ -554,20 +643,6 @@ def algorithmic_bytes(n, primes, limbs):
             "k3_cols_crt": crt, "k3t_cols_crt": crt}
 
 
-def read_profile_traffic(kernel):
-    """DRAM bytes per product recorded from an ncu capture in profiles/<kernel>.md, if any."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.strip().startswith("traffic_bytes_per_product:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
-
-
 def pcie_bandwidth(torch, device, nbytes=256 << 20, reps=4):
     """Pinned host <-> device copy rates (GB/s), each direction alone, CUDA events on a side stream."""
     h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
@@ -741,10 +816,10 @@ def run_ours(args):
         cnt, tot = prof[dom]
         per_launch = alg[dom] * timed_products / cnt
         achieved = per_launch / (tot / cnt / 1000.0) / 1e9
-        traffic = read_profile_traffic(dom)
+        # DRAM bytes come from ncu captures only (a profiler run is never a timed run): not measured here
         roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_src,
-                    "traffic": traffic * timed_products / cnt if traffic else None,
+                    "traffic": None,
                     "algorithmic_bytes_per_launch": per_launch,
                     "algorithmic_bytes_per_product": alg[dom]}
 
@@ -797,12 +872,26 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        from tests import reference_emulation as emu
+
+        cores = host_cores()
         (ca, cb), = host_inputs(n, q, args.seed + 5)
         threads = os.cpu_count() or 1
         v, done, el = cpu_sample(ca, cb, q, args.cpu_seconds, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{done} products (N={n}, {bits}-bit q) in {el:.1f} s through the C restatement of the "
-                         "reference RNS method (oracle/polymul_oracle.c), threads over primes"}
+        port = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": f"{done} products (N={n}, {bits}-bit q) in {el:.1f} s through the C restatement of the "
+                          "reference RNS method (oracle/polymul_oracle.c), threads over primes"}
+        if emu.available() and n <= 32768:
+            # the reference's own kernels, one product per host core at once (the emulation is single-threaded)
+            ev, wall, secs, (ea, eb, ec) = emulated_reference_sample(n, cores, cores, args.seed + 7)
+            if not (ec == oracle.rns_multiply(ea, eb, FHERMA_Q)).all():
+                raise SystemExit("emulated reference disagrees with the oracle")
+            cpu = {"value": ev, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"{cores} products (N={n}, q = 2^868 - 11993087, the form the reference takes) in "
+                             f"{wall:.1f} s through the reference's own rns kernels run by its CPU emulation, one "
+                             "single-threaded process per core", "port": port}
+        else:
+            cpu = port
 
     if rank == 0:
         line = {

@@ -143,6 +143,17 @@ void check_device_errors(const PlanCore& s);
 // and 16 bytes at a time), and 16-byte aligned on the tensor path (tensor maps
 // of a, b and the residue workspace).  Throws PM_ERR_INVALID otherwise.
 void check_device_pointers(const PlanCore& s, const void* a, const void* b, const void* c, const void* workspace);
+// Calls on device pointers run on the caller's current device, which must be the
+// plan's: its tables, twiddles, error word and workspace live there.  Throws
+// PM_ERR_INVALID otherwise (nothing is launched).
+void require_plan_device(const PlanCore& s);
+// Host-buffer calls make the plan's device current for their duration and put
+// the caller's device back afterwards.
+struct DeviceScope {
+    int previous = -1;
+    explicit DeviceScope(int device);
+    ~DeviceScope();
+};
 void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count,
                   uint32_t group, void* workspace, cudaStream_t st);
 void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,

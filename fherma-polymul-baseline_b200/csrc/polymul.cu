@@ -277,8 +277,13 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     if (!q64 || q_limbs == 0) throw Failure(PM_ERR_INVALID, "q is missing");
     if (n_ < 2 || (n_ & (n_ - 1))) throw Failure(PM_ERR_INVALID, "n must be a power of two >= 2");
     if (n_ > uint32_t(kNMax)) throw Failure(PM_ERR_UNSUPPORTED, "n above 65536");
-    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_SPECIAL_FORM | PM_WIDE_NTT))
+    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_CONVERT_SIMT | PM_SPECIAL_FORM | PM_WIDE_NTT))
         throw Failure(PM_ERR_INVALID, "unknown flags");
+    if ((flags_ & PM_CONVERT_TENSOR) && (flags_ & PM_CONVERT_SIMT))
+        throw Failure(PM_ERR_INVALID, "PM_CONVERT_TENSOR and PM_CONVERT_SIMT exclude each other");
+    // no path asked for: the tensor path wherever its 16-byte coefficient rows exist
+    if (!(flags_ & (PM_CONVERT_TENSOR | PM_CONVERT_SIMT | PM_WIDE_NTT)) && coef_limbs_ % 2 == 0)
+        flags_ |= PM_CONVERT_TENSOR;
     q.assign(2 * q_limbs, 0);
     for (uint32_t i = 0; i < q_limbs; ++i) {
         q[2 * i] = uint32_t(q64[i]);
@@ -552,7 +557,28 @@ void check_device_pointers(const PlanCore& s, const void* a, const void* b, cons
         if (at.type == cudaMemoryTypeUnregistered)
             throw Failure(PM_ERR_INVALID, std::string(names[i]) +
                                               " is pageable host memory: pass device, managed or pinned memory");
+        if (at.type == cudaMemoryTypeDevice && at.device != s.device)
+            throw Failure(PM_ERR_INVALID, std::string(names[i]) + " is memory of device " + std::to_string(at.device) +
+                                              ", the plan belongs to device " + std::to_string(s.device));
     }
+}
+
+void require_plan_device(const PlanCore& s) {
+    int device = -1;
+    cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+    if (device != s.device)
+        throw Failure(PM_ERR_INVALID, "the current device is " + std::to_string(device) + ", the plan belongs to device " +
+                                          std::to_string(s.device) + ": make the plan's device current first");
+}
+
+DeviceScope::DeviceScope(int device) {
+    cuda_check(cudaGetDevice(&previous), "cudaGetDevice");
+    if (previous != device) cuda_check(cudaSetDevice(device), "cudaSetDevice");
+}
+
+DeviceScope::~DeviceScope() {
+    int now = -1;
+    if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous) cudaSetDevice(previous);
 }
 
 // A kernel that gave up a bounded wait records it in the plan's error word.
@@ -812,7 +838,7 @@ extern "C" int pm_plan_get_info(const pm_plan* plan, pm_plan_info* info) {
     info->q_bits = s.qbits;
     info->coef_limbs = s.coef_limbs;
     info->primes = s.P;
-    info->convert = s.flags & PM_CONVERT_TENSOR;
+    info->convert = s.wide ? 0u : ((s.flags & PM_CONVERT_TENSOR) ? uint32_t(PM_CONVERT_TENSOR) : uint32_t(PM_CONVERT_SIMT));
     info->reserved = 0;
     info->workspace_bytes = s.workspace_bytes;
     return PM_OK;
@@ -830,6 +856,7 @@ extern "C" int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, 
                            pm_stream stream) {
     if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
     PM_GUARD({
+        pm::require_plan_device(plan->core);
         pm::check_device_pointers(plan->core, a, b, c, workspace);
         pm::launch_product(plan->core, a, b, c, workspace, reinterpret_cast<cudaStream_t>(stream));
     })
@@ -848,6 +875,7 @@ extern "C" int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_
     if (count == 0) return PM_OK;
     PM_GUARD({
         auto& s = plan->core;
+        pm::require_plan_device(s);
         pm::check_device_pointers(s, a, b, c, workspace);
         uint32_t g = pm::group_size(s);
         if (g > count) g = count;
@@ -866,12 +894,18 @@ extern "C" int pm_multiply_batch(pm_plan* plan, const uint64_t* a, const uint64_
 extern "C" int pm_multiply_host_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c,
                                       uint32_t count) {
     if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
-    PM_GUARD(pm::multiply_host_batch(plan->core, a, b, c, count))
+    PM_GUARD({
+        pm::DeviceScope on(plan->core.device);
+        pm::multiply_host_batch(plan->core, a, b, c, count);
+    })
 }
 
 extern "C" int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c) {
     if (!plan || !a || !b || !c) return fail(PM_ERR_INVALID, "NULL argument");
-    PM_GUARD(pm::multiply_host(plan->core, a, b, c))
+    PM_GUARD({
+        pm::DeviceScope on(plan->core.device);
+        pm::multiply_host(plan->core, a, b, c);
+    })
 }
 
 extern "C" int pm_basis_query(uint32_t n, uint32_t q_bits, uint32_t* primes, uint32_t capacity, uint32_t* count) {

@@ -293,7 +293,7 @@ extern "C" int pm_server_create(pm_server** out, const pm_server_config* cfg) {
     if (!out || !cfg) return fail(PM_ERR_INVALID, "NULL argument");
     *out = nullptr;
     if (cfg->slots == 0 || cfg->slots > 64) return fail(PM_ERR_INVALID, "slots must be in [1, 64]");
-    if (cfg->flags & ~uint32_t(PM_CONVERT_TENSOR)) return fail(PM_ERR_INVALID, "unknown flags");
+    if (cfg->flags & ~uint32_t(PM_CONVERT_TENSOR | PM_CONVERT_SIMT)) return fail(PM_ERR_INVALID, "unknown flags");
     PM_SGUARD({
         auto srv = std::make_unique<pm_server>();
         pm::Server& s = srv->s;

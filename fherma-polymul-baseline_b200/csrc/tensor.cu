@@ -88,17 +88,6 @@ void tensor_release(PlanCore& s) {
 }
 
 namespace {
-int sm_count() {
-    static int count = 0;
-    if (!count) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
-        if (!count) count = 148;
-    }
-    return count;
-}
-
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
@@ -150,7 +139,7 @@ void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
     const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
     const int pgs = int((s.P + tc::kConvGroup - 1) / tc::kConvGroup);
     const int items = pgs * int(count) * 2 * (C / Gc);
-    int ctas = sm_count() * s.tune.conv_ctas_per_sm;
+    int ctas = s.sms * s.tune.conv_ctas_per_sm;
     if (ctas > items) ctas = items;
     if (ctas >= pgs) ctas -= ctas % pgs;  // equal numbers of CTAs per prime group (PlanConvWork::range)
     if (ctas < 1) ctas = 1;
@@ -176,7 +165,7 @@ template <int LOGR, int W>
 void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t count, cudaStream_t st) {
     const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
     const int items = int(count) * (C / Gc);
-    int ctas = sm_count() * s.tune.crt_ctas_per_sm;
+    int ctas = s.sms * s.tune.crt_ctas_per_sm;
     if (ctas > items) ctas = items;
     const size_t smem = k3t_smem_bytes<LOGR>();
     // one plan, one q: the reduction is chosen here rather than per coefficient

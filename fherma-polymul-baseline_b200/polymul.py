@@ -25,8 +25,9 @@ PM_ERR_CUDA = 3
 PM_ERR_NO_MEMORY = 4
 PM_ERR_TIMEOUT = 5
 PM_ERR_BUSY = 6
-PM_CONVERT_SIMT = 0
+PM_CONVERT_DEFAULT = 0
 PM_CONVERT_TENSOR = 1
+PM_CONVERT_SIMT = 8
 PM_SPECIAL_FORM = 2
 PM_WIDE_NTT = 4
 
@@ -161,7 +162,9 @@ def selftest_bounded_wait(limit_us):
 class Plan:
     """A product plan for (n, q): basis, CRT constants, workspace, staging."""
 
-    def __init__(self, n, q, coef_limbs=None, tensor=False, special_form=False, wide=False):
+    def __init__(self, n, q, coef_limbs=None, tensor=None, special_form=False, wide=False):
+        """tensor: None lets the library choose (the tensor path when coef_limbs is even),
+        True asks for the tcgen05 conversion/CRT, False for the plain method."""
         self.q = int(q)
         qarr = q_limbs_of(self.q)
         self.n = int(n)
@@ -169,13 +172,20 @@ class Plan:
         self._h = ctypes.c_void_p()
         check(lib().pm_plan_create(ctypes.byref(self._h), self.n,
                                    qarr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(qarr),
-                                   self.coef_limbs, (PM_CONVERT_TENSOR if tensor else PM_CONVERT_SIMT)
+                                   self.coef_limbs, self._convert_flag(tensor)
                                    | (PM_SPECIAL_FORM if special_form else 0) | (PM_WIDE_NTT if wide else 0)))
         info = PlanInfo()
         check(lib().pm_plan_get_info(self._h, ctypes.byref(info)))
         self.info = info
         self.primes = info.primes
         self.workspace_bytes = info.workspace_bytes
+        self.tensor = info.convert == PM_CONVERT_TENSOR
+
+    @staticmethod
+    def _convert_flag(tensor):
+        if tensor is None:
+            return PM_CONVERT_DEFAULT
+        return PM_CONVERT_TENSOR if tensor else PM_CONVERT_SIMT
 
     @property
     def handle(self):

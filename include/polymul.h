@@ -39,10 +39,14 @@ enum pm_status {
     PM_ERR_BUSY = 6         /* admission refused: no slot or device memory free */
 };
 
-/* Residue conversion and CRT implementation. */
+/* Residue conversion and CRT implementation.  With neither PM_CONVERT_TENSOR nor
+ * PM_CONVERT_SIMT a plan takes the tensor-core path whenever coef_limbs is even (16-byte
+ * coefficient rows, which its tensor maps need; the FHERMA point's 14 limbs are), else
+ * the plain method; pm_plan_info.convert says which one it runs. */
 enum pm_flags {
-    PM_CONVERT_SIMT = 0,   /* scalar CUDA-core conversion and CRT (the plain method) */
-    PM_CONVERT_TENSOR = 1, /* exact INT8 digit contractions on the tcgen05 tensor cores */
+    PM_CONVERT_DEFAULT = 0, /* the tensor path where the plan allows it, else the plain method */
+    PM_CONVERT_TENSOR = 1,  /* exact INT8 digit contractions on the tcgen05 tensor cores */
+    PM_CONVERT_SIMT = 8,    /* scalar CUDA-core conversion and CRT (the plain method) */
     /* For a q of the special form 2^k - delta (k >= 80, delta < 2^32, e.g. the FHERMA modulus
      * 2^868 - 11993087; the family the reference's quartic backend targets,
      * quartic/host_setup.h:41-110), reduce the CRT sum by folding 2^k = delta instead of by the
@@ -61,7 +65,7 @@ typedef struct {
     uint32_t q_bits;
     uint32_t coef_limbs;
     uint32_t primes;          /* RNS basis size for (n, q) */
-    uint32_t convert;         /* PM_CONVERT_* the plan runs */
+    uint32_t convert;         /* PM_CONVERT_TENSOR or PM_CONVERT_SIMT: the path the plan runs (0 for PM_WIDE_NTT) */
     uint32_t reserved;
     size_t workspace_bytes;   /* device scratch one product needs (residue planes) */
 } pm_plan_info;
@@ -112,8 +116,10 @@ int pm_plan_destroy(pm_plan* plan);
  * (rns/solve.cu:504-578, launch_rns).
  * Pointers must be device, managed or pinned memory, 8-byte aligned; on the
  * tensor path a, b and workspace 16-byte aligned (cudaMalloc gives 256):
- * otherwise PM_ERR_INVALID, before anything runs.  The same holds for
- * pm_multiply_batch and pm_multiply_noalloc.
+ * otherwise PM_ERR_INVALID, before anything runs.  The call runs on the
+ * current device, which must be the one the plan was created on, and device
+ * pointers must be that device's memory: otherwise PM_ERR_INVALID too.  The
+ * same holds for pm_multiply_batch and pm_multiply_noalloc.
  */
 int pm_multiply(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                 pm_stream stream);
@@ -136,8 +142,9 @@ int pm_batch_workspace_size(const pm_plan* plan, uint32_t count, size_t* bytes);
 /*
  * One product on host memory, synchronous: copy in, multiply, copy out.
  * Pinned (page-locked) buffers are copied directly; pageable ones are staged
- * through the plan's pinned buffers.  Replaces fherma_run (fherma.h:45;
- * rns/solve.cu:721-853).
+ * through the plan's pinned buffers.  Runs on the plan's device whichever
+ * device is current (and leaves the caller's current device as it was).
+ * Replaces fherma_run (fherma.h:45; rns/solve.cu:721-853).
  */
 int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c);
 
@@ -149,8 +156,9 @@ int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64
  * refuses larger ones with PM_ERR_UNSUPPORTED.  For callers that cannot
  * allocate device memory when they multiply.  All calls on a device share the
  * array: calls that overlap on the GPU race.  The first call on each device
- * looks the array's address up (cudaGetSymbolAddress); make that first call
- * before any stream capture.  This entry point has no counterpart in the
+ * (and the first after a cudaDeviceReset, whose new context holds the array at
+ * a new address) looks the array's address up (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  This entry point has no counterpart in the
  * reference, which always multiplies in buffers it allocated in fherma_init.
  */
 int pm_multiply_noalloc(const pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, pm_stream stream);
@@ -160,8 +168,9 @@ int pm_multiply_noalloc(const pm_plan* plan, const uint64_t* a, const uint64_t* 
  * u64 each), synchronous.  The batch is cut into groups that rotate over three
  * streams, so the copies in of one group, the kernels of another and the
  * copies out of a third overlap.  Pinned buffers are copied directly; pageable
- * ones are staged through pinned memory by the calling thread.  No counterpart
- * in the reference (one product per fherma_run).
+ * ones are staged through pinned memory by the calling thread.  Runs on the
+ * plan's device, like pm_multiply_host.  No counterpart in the reference (one
+ * product per fherma_run).
  */
 int pm_multiply_host_batch(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count);
 

@@ -51,7 +51,9 @@ def load_validate(reference):
 
 
 def main():
-    reference = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <reference source tree>")
+    reference = sys.argv[1]
     validate = load_validate(reference)
     points = []
     for n, delta in POINTS:

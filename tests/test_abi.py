@@ -42,6 +42,13 @@ def test_invalid_arguments_fail_before_cuda():
     assert e.value.status == polymul.PM_ERR_UNSUPPORTED
     with pytest.raises(polymul.PolymulError):
         polymul.Plan(32, (1 << 868) - 11993087, coef_limbs=13)
+    # the two conversion paths exclude each other; unknown flag bits are refused
+    for flags in (polymul.PM_CONVERT_TENSOR | polymul.PM_CONVERT_SIMT, 1 << 12):
+        h = ctypes.c_void_p()
+        qa = polymul.q_limbs_of(101)
+        status = polymul.lib().pm_plan_create(ctypes.byref(h), 32, qa.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                              1, 1, flags)
+        assert status == polymul.PM_ERR_INVALID and not h.value
     for limit in (0, 2_000_001):
         with pytest.raises(polymul.PolymulError) as e:
             polymul.selftest_bounded_wait(limit)
