@@ -413,6 +413,58 @@ def run_plain(args, torch, plan, A, Bv, Cv, stream, batched_value):
             "products": {"device": K * args.steps, "host": H * reps}}
 
 
+def run_fherma_drop_in(args, q, cases=24):
+    """The drop-in call itself: fherma_run on the harness's own std::vector inputs (pageable
+    memory), timed by the harness around each call, as the reference's published number is.
+    Two harnesses run the same point directory of `cases` products at the bench's N and q:
+    this repository's runner (polymul_solution) and the reference's unmodified main.cpp linked
+    against libfherma_polymul.so (oracle/_ref/fherma_main, when it was built).  Per-case
+    seconds come from their results.json; c.bin files are checked against the oracle on two
+    cases."""
+    import tempfile
+
+    import numpy as np
+
+    from oracle import oracle
+    from tests import reference_emulation as emu
+
+    n, limbs = args.ring, (args.bits + 63) // 64
+    if limbs != 14:
+        return None
+    harnesses = {"polymul_solution": os.path.join(PKG, "polymul_solution"),
+                 "reference_main_cpp": os.path.join(ROOT, "oracle", "_ref", "fherma_main")}
+    rng = np.random.default_rng(args.seed + 97)
+    from tests.helpers import uniform_below
+
+    pairs = [(uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)) for _ in range(4)]
+    out = {"cases": cases, "n": n, "api": "fherma_run (fherma.h:45) on std::vector inputs, harness-timed"}
+    with tempfile.TemporaryDirectory() as tmp:
+        # the point directory format the reference's harness reads (main.cpp:137-208); 4 distinct
+        # input pairs cycled over the cases
+        emu.write_point(tmp, n, q, [pairs[k % len(pairs)] for k in range(cases)])
+        for name, exe in harnesses.items():
+            if not os.path.exists(exe):
+                continue
+            res_dir = os.path.join(tmp, "out")
+            r = subprocess.run([exe, tmp], capture_output=True, text=True, timeout=600)
+            if r.returncode != 0:
+                out[name] = {"error": r.stderr[-300:]}
+                continue
+            got, secs = emu.read_results(tmp, cases, n)
+            for k in (0, 1):
+                a, b = pairs[k]
+                if not (got[k] == oracle.rns_multiply(a, b, q)).all():
+                    raise SystemExit(f"{name}: fherma_run output differs from the oracle")
+            us = sorted(1e6 * x for x in secs[1:])  # the first call pays one-time staging set-up
+            pick = lambda f: us[min(len(us) - 1, int(f * (len(us) - 1) + 0.5))]  # noqa: E731
+            out[name] = {"p50_us": pick(0.5), "p99_us": pick(0.99), "min_us": us[0], "mean_us": sum(us) / len(us),
+                         "first_call_us": 1e6 * secs[0]}
+            import shutil
+
+            shutil.rmtree(res_dir, ignore_errors=True)
+    return out
+
+
 def run_special(args, torch, polymul, tuning):
     """The reference's FHERMA modulus q = 2^868 - 11993087, a special-form prime: device products/s
     with the folding reduction (PM_SPECIAL_FORM) and with the general one (the default), same
@@ -431,7 +483,7 @@ def run_special(args, torch, polymul, tuning):
         plan = polymul.Plan(n, q, coef_limbs=limbs, tensor=(args.path == "tensor"), special_form=special)
         if tuning and "row_radix" in tuning:
             plan.set_tuning(tuning["row_radix"], tuning["conv_ctas_per_sm"], tuning["crt_ctas_per_sm"],
-                            tuning["group"], tuning["row_persistent"])
+                            tuning["group"], tuning["row_persistent"], tuning["conv_whole_basis"])
         elif args.group:
             plan.set_tuning(group=args.group)
         C = torch.empty_like(A)
@@ -760,6 +812,8 @@ def run_ours(args):
     value = total_products / (ms / 1000.0)
 
     plain = run_plain(args, torch, plan, A, Bv, Cv, stream, value / world)
+    if world == 1:
+        plain["fherma_run"] = run_fherma_drop_in(args, q)
 
     # end to end through the C ABI host-buffer call, pinned host memory
     # the whole batch on one GPU; 64 products a rank when several ranks share the host's pinned memory

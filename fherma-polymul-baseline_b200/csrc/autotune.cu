@@ -5,7 +5,9 @@
 //   row_radix_log    K2 register passes of radix 4, 8 or 16 (more passes with
 //                    less register state, or fewer shared-memory exchanges;
 //                    radix 16 in the persistent kernel, rows of >= 1024 values);
-//   conv_ctas_per_sm persistent CTAs of the tensor conversion per SM;
+//   conv_whole_basis the tensor conversion taking a coefficient tile through every
+//                    prime at once (K1W) or once per group of 16 primes (K1T);
+//   conv_ctas_per_sm persistent CTAs of K1T per SM;
 //   crt_ctas_per_sm  persistent CTAs of the tensor CRT per SM;
 //   row_persistent   K2 as one CTA per row, or as the persistent kernel that
 //                    stages each row's twiddles once per group and prefetches;
@@ -121,7 +123,13 @@ Tuning autotune(PlanCore& s, uint32_t reps, double* us_per_product) {
         }
     }
     if (s.flags & PM_CONVERT_TENSOR) {
+        {
+            Tuning t = best;
+            t.conv_whole_basis = !best.conv_whole_basis;
+            consider(t);
+        }
         for (int k : {2, 3, 4}) {
+            if (best.conv_whole_basis) break;  // fixed at two CTAs per SM
             Tuning t = best;
             t.conv_ctas_per_sm = k;
             if (k != best.conv_ctas_per_sm) consider(t);
@@ -163,6 +171,7 @@ extern "C" int pm_plan_autotune(pm_plan* plan, uint32_t reps, pm_tuning* chosen)
             chosen->crt_ctas_per_sm = uint32_t(t.crt_ctas_per_sm);
             chosen->group = t.group;
             chosen->row_persistent = t.row_persistent ? 1u : 0u;
+            chosen->conv_whole_basis = t.conv_whole_basis ? 1u : 0u;
             chosen->us_per_product = us;
         }
         return PM_OK;
@@ -181,12 +190,14 @@ extern "C" int pm_plan_set_tuning(pm_plan* plan, const pm_tuning* t) {
         return pm::fail(PM_ERR_INVALID, "CTAs per SM out of range");
     if (t->group > pm::kMaxGroup) return pm::fail(PM_ERR_INVALID, "group above 256");
     if (t->row_persistent > 1) return pm::fail(PM_ERR_INVALID, "row_persistent must be 0 or 1");
+    if (t->conv_whole_basis > 1) return pm::fail(PM_ERR_INVALID, "conv_whole_basis must be 0 or 1");
     pm::Tuning& u = plan->core.tune;
     u.row_radix_log = t->row_radix == 4 ? 2 : (t->row_radix == 8 ? 3 : 4);
     u.conv_ctas_per_sm = int(t->conv_ctas_per_sm);
     u.crt_ctas_per_sm = int(t->crt_ctas_per_sm);
     u.group = t->group;
     u.row_persistent = t->row_persistent != 0;
+    u.conv_whole_basis = t->conv_whole_basis != 0;
     u.tuned = true;
     return PM_OK;
 }

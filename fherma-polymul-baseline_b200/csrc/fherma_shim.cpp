@@ -54,12 +54,20 @@ fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
     const size_t words = size_t(s.n) * s.words;
     if (in.a.data.size() != words || in.b.data.size() != words)
         throw std::runtime_error("fherma_run: inputs must be N x L words");
+    // inputs staged and everything queued; the output tensor is allocated while the GPU runs
+    int st = pm_multiply_host_begin(s.plan, reinterpret_cast<const uint64_t*>(in.a.data.data()),
+                                    reinterpret_cast<const uint64_t*>(in.b.data.data()));
+    if (st != PM_OK) raise(st, "fherma_run");
     fherma::Outputs out;
-    out.c.shape = {int64_t(s.n), int64_t(s.words)};
-    out.c.data.resize(words);
-    const int st = pm_multiply_host(s.plan, reinterpret_cast<const uint64_t*>(in.a.data.data()),
-                                    reinterpret_cast<const uint64_t*>(in.b.data.data()),
-                                    reinterpret_cast<uint64_t*>(out.c.data.data()));
+    try {
+        out.c.shape = {int64_t(s.n), int64_t(s.words)};
+        out.c.data.resize(words);
+    } catch (...) {
+        std::vector<uint32_t> sink(words);  // the open product still needs somewhere to land
+        pm_multiply_host_end(s.plan, reinterpret_cast<uint64_t*>(sink.data()));
+        throw;
+    }
+    st = pm_multiply_host_end(s.plan, reinterpret_cast<uint64_t*>(out.c.data.data()));
     if (st != PM_OK) raise(st, "fherma_run");
     return out;
 }

@@ -1,0 +1,282 @@
+// The single-product host-buffer call (pm_multiply_host, the fherma_run of the
+// drop-in), pipelined.
+//
+// The caller's a, b, c are usually pageable (the harness's std::vector
+// tensors), which the GPU cannot read: every byte goes through pinned staging.
+// Done serially that is two host copies of 3.7 MB, an H2D of 7.3 MB, the
+// kernels, a D2H of 3.7 MB and a host copy of 3.7 MB, one after the other.
+// Here:
+//   - the inputs are cut into pieces; a small pool of host threads copies
+//     piece k into pinned staging (non-temporal stores) and queues its H2D at
+//     once, so staging, the PCIe transfer and the other threads' copies
+//     overlap (the reference gets the same overlap from its copy pool and
+//     4-chunk input pipeline, host_copy_pool.h, input_pipeline.h:12-54,
+//     rns/solve.cu:731-761);
+//   - the kernels follow on the same stream; the product comes back in
+//     pieces, each with an event, and the pool copies piece k out as soon as
+//     its event fires, while later pieces are still on the link;
+//   - the call is split (begin / end) so that a caller can do its own work --
+//     the drop-in allocates the output tensor -- while the GPU runs.
+// Pinned caller buffers skip the staging: their pieces are copied directly.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <immintrin.h>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/polymul.h"
+#include "pm_internal.h"
+
+namespace pm {
+
+namespace {
+
+// dst 32-byte aligned, bytes a multiple of 32: 256-bit loads, streaming stores
+__attribute__((target("avx2"))) void stream_copy_avx2(void* dst, const void* src, size_t bytes) {
+    auto* d = static_cast<__m256i*>(dst);
+    auto* s = static_cast<const __m256i*>(src);
+    const size_t n = bytes / 32;
+    size_t k = 0;
+    for (; k + 4 <= n; k += 4) {
+        const __m256i x0 = _mm256_loadu_si256(s + k), x1 = _mm256_loadu_si256(s + k + 1);
+        const __m256i x2 = _mm256_loadu_si256(s + k + 2), x3 = _mm256_loadu_si256(s + k + 3);
+        _mm256_stream_si256(d + k, x0);
+        _mm256_stream_si256(d + k + 1, x1);
+        _mm256_stream_si256(d + k + 2, x2);
+        _mm256_stream_si256(d + k + 3, x3);
+    }
+    for (; k < n; ++k) _mm256_stream_si256(d + k, _mm256_loadu_si256(s + k));
+    _mm_sfence();
+}
+
+bool have_avx2() {
+    static const bool yes = __builtin_cpu_supports("avx2");
+    return yes;
+}
+
+// Copy that does not pull the destination into the cache when it can.
+void host_copy(void* dst, const void* src, size_t bytes) {
+    const uintptr_t d = reinterpret_cast<uintptr_t>(dst);
+    if (have_avx2() && bytes >= 4096) {
+        const size_t head = (32 - (d & 31)) & 31;
+        if (head) std::memcpy(dst, src, head);
+        const size_t body = (bytes - head) & ~size_t(31);
+        stream_copy_avx2(static_cast<uint8_t*>(dst) + head, static_cast<const uint8_t*>(src) + head, body);
+        const size_t tail = bytes - head - body;
+        if (tail) std::memcpy(static_cast<uint8_t*>(dst) + head + body, static_cast<const uint8_t*>(src) + head + body, tail);
+        return;
+    }
+    std::memcpy(dst, src, bytes);
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+// Persistent host threads that run the pieces of one job; the calling thread
+// takes pieces too.  Idle workers spin for a short while (back-to-back calls
+// find them awake), then sleep on a condition variable.
+class CopyPool {
+public:
+    explicit CopyPool(int threads) {
+        for (int t = 0; t < threads; ++t) workers_.emplace_back([this] { loop(); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            stop_ = true;
+            ++generation_;
+        }
+        cv_.notify_all();
+        for (auto& w : workers_) w.join();
+    }
+    int threads() const { return int(workers_.size()); }
+
+    // Runs f(k) for k in [0, pieces) on the workers and the caller; returns when
+    // all are done and no worker is still inside the job.  The first exception a
+    // piece throws is rethrown here.
+    void run(int pieces, const std::function<void(int)>& f) {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            job_ = &f;
+            pieces_ = pieces;
+            next_.store(0);
+            done_.store(0);
+            error_ = nullptr;
+            generation_.fetch_add(1, std::memory_order_release);
+        }
+        cv_.notify_all();
+        work(&f, pieces);
+        while (done_.load(std::memory_order_acquire) < pieces) _mm_pause();
+        // no worker joins from here on (they join under the lock while job_ is set); the ones
+        // that joined find no piece left and leave before the next job resets the counters
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            job_ = nullptr;
+        }
+        while (active_.load(std::memory_order_acquire) > 0) _mm_pause();
+        if (error_) std::rethrow_exception(error_);
+    }
+
+private:
+    void work(const std::function<void(int)>* f, int pieces) {
+        for (int k = next_.fetch_add(1); k < pieces; k = next_.fetch_add(1)) {
+            try {
+                (*f)(k);
+            } catch (...) {
+                std::lock_guard<std::mutex> lock(m_);
+                if (!error_) error_ = std::current_exception();
+            }
+            done_.fetch_add(1, std::memory_order_release);
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        while (true) {
+            // a short spin catches the next call of a caller that multiplies in a loop
+            const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(200);
+            while (generation_.load(std::memory_order_acquire) == seen && std::chrono::steady_clock::now() < spin_until)
+                _mm_pause();
+            std::unique_lock<std::mutex> lock(m_);
+            cv_.wait(lock, [&] { return generation_.load() != seen; });
+            seen = generation_.load();
+            if (stop_) return;
+            if (!job_) continue;  // that job is over already
+            const std::function<void(int)>* f = job_;
+            const int pieces = pieces_;
+            active_.fetch_add(1, std::memory_order_acq_rel);
+            lock.unlock();
+            work(f, pieces);
+            active_.fetch_sub(1, std::memory_order_acq_rel);
+        }
+    }
+
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::atomic<uint64_t> generation_{0};
+    const std::function<void(int)>* job_ = nullptr;
+    int pieces_ = 0;
+    std::atomic<int> next_{0}, done_{0}, active_{0};
+    std::exception_ptr error_;
+    bool stop_ = false;
+};
+
+namespace {
+constexpr int kInPieces = 8;   // pieces of each input polynomial
+constexpr int kOutPieces = 8;  // pieces of the product
+
+int pool_threads() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    int t = hw ? int(hw / 2) : 4;
+    if (t > 8) t = 8;
+    if (t < 1) t = 1;
+    return t;
+}
+
+// piece k of `bytes` cut into `pieces` runs of 64-byte multiples
+void piece(size_t bytes, int pieces, int k, size_t* off, size_t* len) {
+    const size_t unit = ((bytes + pieces - 1) / pieces + 63) & ~size_t(63);
+    *off = std::min(bytes, unit * size_t(k));
+    *len = std::min(bytes, *off + unit) - *off;
+}
+}  // namespace
+
+HostCall::~HostCall() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& e : out_ready)
+        if (e) cudaEventDestroy(e);
+    cudaFree(d_io);
+    cudaFreeHost(h_stage);
+}
+
+void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* direct_out) {
+    if (!s.host) s.host = std::make_unique<HostCall>();
+    HostCall& h = *s.host;
+    if (h.pending) throw Failure(PM_ERR_BUSY, "a host-buffer product of this plan is still open: end it first");
+    if (!h.d_io) {
+        h.stream = s.stream;
+        cuda_check(cudaMalloc(&h.d_io, 3 * s.io_bytes), "allocate plan I/O buffers");
+        // staging for a, b, c, then one word the device error flag is copied into
+        cuda_check(cudaMallocHost(&h.h_stage, 3 * s.io_bytes + 64), "allocate pinned staging");
+        h.out_ready.assign(kOutPieces, nullptr);
+        for (auto& e : h.out_ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "output events");
+    }
+    if (!h.pool) h.pool = std::make_unique<CopyPool>(pool_threads());
+    const size_t io = s.io_bytes;
+    uint8_t* dev = static_cast<uint8_t*>(h.d_io);
+    uint8_t* stage = static_cast<uint8_t*>(h.h_stage);
+    const uint8_t* src[2] = {reinterpret_cast<const uint8_t*>(a), reinterpret_cast<const uint8_t*>(b)};
+    const bool pinned[2] = {is_pinned(a), is_pinned(b)};
+    // every input piece: stage it (pageable source), then queue its H2D right away
+    h.pool->run(2 * kInPieces, [&](int k) {
+        const int poly = k / kInPieces;
+        size_t off, len;
+        piece(io, kInPieces, k % kInPieces, &off, &len);
+        if (!len) return;
+        const uint8_t* from = src[poly] + off;
+        if (!pinned[poly]) {
+            host_copy(stage + poly * io + off, from, len);
+            from = stage + poly * io + off;
+        }
+        cuda_check(cudaMemcpyAsync(dev + poly * io + off, from, len, cudaMemcpyHostToDevice, h.stream), "copy in");
+    });
+    launch_product(s, reinterpret_cast<const uint64_t*>(dev), reinterpret_cast<const uint64_t*>(dev + io),
+                   reinterpret_cast<uint64_t*>(dev + 2 * io), nullptr, h.stream);
+    // a pinned output takes the product directly; otherwise it lands in the staging
+    h.direct_out = direct_out && is_pinned(direct_out) ? reinterpret_cast<uint8_t*>(direct_out) : nullptr;
+    uint8_t* land = h.direct_out ? h.direct_out : stage + 2 * io;
+    for (int k = 0; k < kOutPieces; ++k) {
+        size_t off, len;
+        piece(io, kOutPieces, k, &off, &len);
+        if (len) cuda_check(cudaMemcpyAsync(land + off, dev + 2 * io + off, len, cudaMemcpyDeviceToHost, h.stream), "copy out");
+        cuda_check(cudaEventRecord(h.out_ready[k], h.stream), "output event");
+    }
+    // the error word rides on the same stream: no second round trip after the product
+    cuda_check(cudaMemcpyAsync(stage + 3 * io, s.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, h.stream),
+               "read error word");
+    h.pending = true;
+}
+
+void multiply_host_end(PlanCore& s, uint64_t* c) {
+    if (!s.host || !s.host->pending) throw Failure(PM_ERR_INVALID, "no host-buffer product of this plan is open");
+    HostCall& h = *s.host;
+    h.pending = false;
+    const size_t io = s.io_bytes;
+    uint8_t* stage = static_cast<uint8_t*>(h.h_stage);
+    uint8_t* dst = reinterpret_cast<uint8_t*>(c);
+    if (h.direct_out && h.direct_out != dst)
+        throw Failure(PM_ERR_INVALID, "the product was directed to another output buffer at the start of the call");
+    // each product piece leaves the staging as soon as it has landed
+    if (!h.direct_out)
+        h.pool->run(kOutPieces, [&](int k) {
+            size_t off, len;
+            piece(io, kOutPieces, k, &off, &len);
+            cuda_check(cudaEventSynchronize(h.out_ready[k]), "product");
+            if (len) host_copy(dst + off, stage + 2 * io + off, len);
+        });
+    cuda_check(cudaStreamSynchronize(h.stream), "product");
+    uint32_t herr = 0;
+    std::memcpy(&herr, stage + 3 * io, sizeof herr);
+    if (herr) check_device_errors(s);
+}
+
+void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c) {
+    multiply_host_begin(s, a, b, c);
+    multiply_host_end(s, c);
+}
+
+}  // namespace pm

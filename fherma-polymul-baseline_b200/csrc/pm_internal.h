@@ -63,6 +63,20 @@ struct PipelineSlot {
     ~PipelineSlot();
 };
 
+// The single-product host-buffer call (host_call.cu): pinned staging, device
+// copies of a, b, c, a host copy pool and the events of the product's pieces.
+class CopyPool;
+struct HostCall {
+    cudaStream_t stream = nullptr;  // the plan's stream
+    void* d_io = nullptr;           // a, b, c on the device
+    void* h_stage = nullptr;        // pinned a, b, c and the error word
+    std::vector<cudaEvent_t> out_ready;
+    std::unique_ptr<CopyPool> pool;
+    bool pending = false;           // between multiply_host_begin and multiply_host_end
+    uint8_t* direct_out = nullptr;  // pinned caller output the product lands in directly, or null
+    ~HostCall();
+};
+
 // Largest launch group by default, and the largest a caller may set.
 constexpr uint32_t kMaxDefaultGroup = 128;
 constexpr uint32_t kMaxGroup = 256;
@@ -73,6 +87,7 @@ struct Tuning {
     int conv_ctas_per_sm = 3;  // K1T persistent CTAs per SM (up to four fit; three measured fastest)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
     bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)
+    bool conv_whole_basis = true;  // tensor conversion: one pass of a tile over every prime (K1W) or per group (K1T)
     uint32_t group = 0;        // products per launch group in batches (0: up to ~2 GB of residues, <= 128)
     bool tuned = false;
 };
@@ -110,8 +125,7 @@ struct PlanCore {
     uint32_t batch_work_group = 0;
     size_t workspace_bytes = 0;
     size_t io_bytes = 0;           // bytes of one polynomial
-    void* d_io = nullptr;          // a, b, c device copies for the host-buffer call
-    void* h_stage = nullptr;       // pinned staging for pageable host buffers
+    std::unique_ptr<HostCall> host;  // the host-buffer call's buffers and copy threads (first use)
     cudaStream_t stream = nullptr;
     // tensor path constants
     uint8_t* d_crt_weights = nullptr;
@@ -159,6 +173,10 @@ void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint6
 void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, void* workspace,
                     cudaStream_t st);
 void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c);
+// the same call in two halves: begin stages a, b and queues everything on the plan's
+// stream; end copies the product out (direct_out: a pinned c the product may land in)
+void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* direct_out = nullptr);
+void multiply_host_end(PlanCore& s, uint64_t* c);
 void multiply_host_batch(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c, uint32_t count);
 
 // direct wide-modulus NTT (wide.cu)

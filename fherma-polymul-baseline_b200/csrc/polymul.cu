@@ -267,8 +267,7 @@ PlanCore::~PlanCore() {
     cudaFree(d_err);
     cudaFree(d_work);
     cudaFree(d_batch_work);
-    cudaFree(d_io);
-    cudaFreeHost(h_stage);
+    host.reset();
     if (stream) cudaStreamDestroy(stream);
     cudaSetDevice(previous);
 }
@@ -631,51 +630,6 @@ void launch_product(const PlanCore& s, const uint64_t* a, const uint64_t* b, uin
     launch_batch(s, a, b, c, 1, 1, workspace ? workspace : s.d_work, st);
 }
 
-// Host buffers: pinned memory is copied directly; pageable memory is staged
-// through the plan's pinned buffer (one memcpy each way).
-void multiply_host(PlanCore& s, const uint64_t* a, const uint64_t* b, uint64_t* c) {
-    if (!s.d_io) {
-        cuda_check(cudaMalloc(&s.d_io, 3 * s.io_bytes), "allocate plan I/O buffers");
-        // staging for a, b, c, then one word the device error flag is copied into
-        cuda_check(cudaMallocHost(&s.h_stage, 3 * s.io_bytes + 16), "allocate pinned staging");
-    }
-    auto pinned = [](const void* p) {
-        cudaPointerAttributes at{};
-        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        return at.type == cudaMemoryTypeHost;
-    };
-    uint8_t* dev = static_cast<uint8_t*>(s.d_io);
-    uint8_t* stage = static_cast<uint8_t*>(s.h_stage);
-    const bool pa = pinned(a), pb = pinned(b), pc = pinned(c);
-    const void* src_a = a;
-    const void* src_b = b;
-    if (!pa) {
-        std::memcpy(stage, a, s.io_bytes);
-        src_a = stage;
-    }
-    if (!pb) {
-        std::memcpy(stage + s.io_bytes, b, s.io_bytes);
-        src_b = stage + s.io_bytes;
-    }
-    cuda_check(cudaMemcpyAsync(dev, src_a, s.io_bytes, cudaMemcpyHostToDevice, s.stream), "copy a to device");
-    cuda_check(cudaMemcpyAsync(dev + s.io_bytes, src_b, s.io_bytes, cudaMemcpyHostToDevice, s.stream),
-               "copy b to device");
-    launch_product(s, reinterpret_cast<const uint64_t*>(dev), reinterpret_cast<const uint64_t*>(dev + s.io_bytes),
-                   reinterpret_cast<uint64_t*>(dev + 2 * s.io_bytes), nullptr, s.stream);
-    void* dst = pc ? static_cast<void*>(c) : static_cast<void*>(stage + 2 * s.io_bytes);
-    cuda_check(cudaMemcpyAsync(dst, dev + 2 * s.io_bytes, s.io_bytes, cudaMemcpyDeviceToHost, s.stream),
-               "copy c to host");
-    // the error word rides on the same stream: no second round trip after the product
-    uint32_t* herr = reinterpret_cast<uint32_t*>(stage + 3 * s.io_bytes);
-    cuda_check(cudaMemcpyAsync(herr, s.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream), "read error word");
-    cuda_check(cudaStreamSynchronize(s.stream), "product");
-    if (*herr) check_device_errors(s);
-    if (!pc) std::memcpy(c, stage + 2 * s.io_bytes, s.io_bytes);
-}
-
 // ---------------------------------------------------------------------------
 // host batches: chunks of `group` products rotate over three slots, each with
 // its own stream, device buffers and workspace, so one slot's H2D, another's
@@ -905,6 +859,22 @@ extern "C" int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t
     PM_GUARD({
         pm::DeviceScope on(plan->core.device);
         pm::multiply_host(plan->core, a, b, c);
+    })
+}
+
+extern "C" int pm_multiply_host_begin(pm_plan* plan, const uint64_t* a, const uint64_t* b) {
+    if (!plan || !a || !b) return fail(PM_ERR_INVALID, "NULL argument");
+    PM_GUARD({
+        pm::DeviceScope on(plan->core.device);
+        pm::multiply_host_begin(plan->core, a, b);
+    })
+}
+
+extern "C" int pm_multiply_host_end(pm_plan* plan, uint64_t* c) {
+    if (!plan || !c) return fail(PM_ERR_INVALID, "NULL argument");
+    PM_GUARD({
+        pm::DeviceScope on(plan->core.device);
+        pm::multiply_host_end(plan->core, c);
     })
 }
 

@@ -14,6 +14,7 @@
 #include "pm_internal.h"
 #include "tc_ptx.cuh"
 #include "tensor_kernels.cuh"
+#include "convert_tile.cuh"
 
 namespace pm {
 
@@ -161,6 +162,40 @@ void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
                                                              s.basis->d_tw_fwd, s.d_err);
 }
 
+// the whole basis per tile: two CTAs per SM, contiguous runs of items
+template <int LOGR>
+void launch_k1w(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, uint32_t count,
+                cudaStream_t st) {
+    const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
+    const int items = int(count) * 2 * (C / Gc);
+    int ctas = s.sms * 2;
+    if (ctas > items) ctas = items;
+    const size_t smem = k1w_smem_bytes();
+    cuda_check(cudaFuncSetAttribute(k1w_convert<LOGR, PlanTileWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(smem)),
+               "K1W shared memory");
+    PlanTileWork w;
+    w.map_a = coefficient_map(s, a, count);
+    w.map_b = coefficient_map(s, b, count);
+    w.work = work;
+    w.ws_bstride = s.workspace_bytes / 4;
+    w.n = int(s.n);
+    w.logC = int(s.logC);
+    w.P = int(s.P);
+    w.count = int(count);
+    k1w_convert<LOGR, PlanTileWork><<<ctas, tc::kWideThreads, smem, st>>>(w, s.basis->d_pc, s.basis->d_conv_weights,
+                                                                        s.basis->d_tw_fwd, s.d_err);
+}
+
+template <int LOGR>
+void launch_conversion(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, uint32_t count,
+                       cudaStream_t st) {
+    if (s.tune.conv_whole_basis)
+        launch_k1w<LOGR>(s, a, b, work, count, st);
+    else
+        launch_k1t<LOGR>(s, a, b, work, count, st);
+}
+
 template <int LOGR, int W>
 void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t count, cudaStream_t st) {
     const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
@@ -214,11 +249,11 @@ void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint
     {
         ProfileScope prof("k1t_convert_cols", st);
         switch (s.logR) {
-            case 0: launch_k1t<0>(s, a, b, work, count, st); break;
-            case 1: launch_k1t<1>(s, a, b, work, count, st); break;
-            case 2: launch_k1t<2>(s, a, b, work, count, st); break;
-            case 3: launch_k1t<3>(s, a, b, work, count, st); break;
-            default: launch_k1t<4>(s, a, b, work, count, st); break;
+            case 0: launch_conversion<0>(s, a, b, work, count, st); break;
+            case 1: launch_conversion<1>(s, a, b, work, count, st); break;
+            case 2: launch_conversion<2>(s, a, b, work, count, st); break;
+            case 3: launch_conversion<3>(s, a, b, work, count, st); break;
+            default: launch_conversion<4>(s, a, b, work, count, st); break;
         }
     }
     {

@@ -49,7 +49,7 @@ class PlanInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("row_radix", ctypes.c_uint32), ("conv_ctas_per_sm", ctypes.c_uint32),
                 ("crt_ctas_per_sm", ctypes.c_uint32), ("group", ctypes.c_uint32), ("row_persistent", ctypes.c_uint32),
-                ("us_per_product", ctypes.c_double)]
+                ("conv_whole_basis", ctypes.c_uint32), ("us_per_product", ctypes.c_double)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -78,6 +78,8 @@ def lib():
         L.pm_plan_destroy.argtypes = [vp]
         L.pm_multiply.argtypes = [vp, vp, vp, vp, vp, vp]
         L.pm_multiply_host.argtypes = [vp, vp, vp, vp]
+        L.pm_multiply_host_begin.argtypes = [vp, vp, vp]
+        L.pm_multiply_host_end.argtypes = [vp, vp]
         L.pm_multiply_host_batch.argtypes = [vp, vp, vp, vp, u32]
         L.pm_multiply_batch.argtypes = [vp, vp, vp, vp, u32, vp, ctypes.c_size_t, vp]
         L.pm_batch_workspace_size.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_size_t)]
@@ -221,6 +223,17 @@ class Plan:
         check(lib().pm_multiply_host(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
         return c
 
+    def multiply_host_begin(self, a, b):
+        """First half of multiply_host: stage a, b and queue the product; returns at once."""
+        a, b = self._shape_ok(a), self._shape_ok(b)
+        check(lib().pm_multiply_host_begin(self._h, a.ctypes.data, b.ctypes.data))
+
+    def multiply_host_end(self, out=None):
+        """Second half: wait for the product and copy it out."""
+        c = np.empty((self.n, self.coef_limbs), dtype=np.uint64) if out is None else out
+        check(lib().pm_multiply_host_end(self._h, c.ctypes.data))
+        return c
+
     def multiply_host_ptr(self, a_ptr, b_ptr, c_ptr):
         """Same on raw host pointers (e.g. pinned torch tensors); synchronous."""
         check(lib().pm_multiply_host(self._h, a_ptr, b_ptr, c_ptr))
@@ -231,8 +244,9 @@ class Plan:
         check(lib().pm_plan_autotune(self._h, reps, ctypes.byref(t)))
         return {name: getattr(t, name) for name, _ in Tuning._fields_}
 
-    def set_tuning(self, row_radix=16, conv_ctas_per_sm=3, crt_ctas_per_sm=2, group=0, row_persistent=1):
-        t = Tuning(row_radix, conv_ctas_per_sm, crt_ctas_per_sm, group, row_persistent, 0.0)
+    def set_tuning(self, row_radix=16, conv_ctas_per_sm=3, crt_ctas_per_sm=2, group=0, row_persistent=1,
+                   conv_whole_basis=1):
+        t = Tuning(row_radix, conv_ctas_per_sm, crt_ctas_per_sm, group, row_persistent, conv_whole_basis, 0.0)
         check(lib().pm_plan_set_tuning(self._h, ctypes.byref(t)))
 
     def multiply_host_batch(self, a, b, out=None):

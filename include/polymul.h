@@ -92,6 +92,9 @@ typedef struct {
                                    128 products; at most 256) */
     uint32_t row_persistent;    /* 1: rows of >= 1024 values by the persistent kernel that stages a row's
                                    twiddles once per group and prefetches rows; 0: one CTA per row */
+    uint32_t conv_whole_basis;  /* tensor conversion: 1 takes each coefficient tile through all primes at once
+                                   (weights of the whole basis resident, 2 CTAs per SM; conv_ctas_per_sm
+                                   unused); 0 runs it once per group of 16 primes */
     double us_per_product;      /* device time the autotuner measured (-1: taken from its cache) */
 } pm_tuning;
 
@@ -147,6 +150,21 @@ int pm_batch_workspace_size(const pm_plan* plan, uint32_t count, size_t* bytes);
  * Replaces fherma_run (fherma.h:45; rns/solve.cu:721-853).
  */
 int pm_multiply_host(pm_plan* plan, const uint64_t* a, const uint64_t* b, uint64_t* c);
+
+/*
+ * pm_multiply_host in two halves, so that the caller can do its own work
+ * while the GPU runs (the drop-in fherma_run allocates its output tensor
+ * there).  begin copies a and b in -- host threads stage pageable pieces
+ * while earlier pieces cross the link -- and queues the kernels and the copy
+ * back; a and b may be reused when it returns.  end copies the product into
+ * c piece by piece as the pieces land and returns the call's status (a wait
+ * that timed out on the device: PM_ERR_TIMEOUT).  One product per plan may be
+ * open at a time (PM_ERR_BUSY otherwise); every begin needs its end.  Same
+ * role as the reference's overlapped input pipeline and output allocation in
+ * fherma_run (rns/solve.cu:729-803, input_pipeline.h:12-54).
+ */
+int pm_multiply_host_begin(pm_plan* plan, const uint64_t* a, const uint64_t* b);
+int pm_multiply_host_end(pm_plan* plan, uint64_t* c);
 
 /*
  * One product, like pm_multiply, but the call allocates nothing: no

@@ -214,17 +214,19 @@ def test_tunings_do_not_change_results(cuda, path, n):
     b = torch.from_numpy(np.stack([uniform_below(rng, q, n, 14) for _ in range(count)]).view(np.int64)).cuda()
     ref = None
     with make_plan(path, n, q, 14) as p:
-        shapes = [(8, 4, 2, 0, 1), (4, 4, 2, 0, 1), (8, 2, 1, 1, 1), (4, 3, 1, 2, 1), (8, 4, 2, 5, 1),
-                  (8, 4, 2, 0, 0), (4, 4, 2, 3, 0), (8, 4, 2, 3, 1), (16, 3, 2, 0, 1), (16, 3, 2, 3, 1),
-                  (16, 3, 2, 2, 0)]
-        for radix, conv, crt, group, persistent in shapes:
-            p.set_tuning(radix, conv, crt, group, persistent)
+        # (row radix, K1T CTAs per SM, K3T CTAs per SM, group, persistent rows, whole-basis conversion)
+        shapes = [(8, 4, 2, 0, 1, 0), (4, 4, 2, 0, 1, 0), (8, 2, 1, 1, 1, 0), (4, 3, 1, 2, 1, 0), (8, 4, 2, 5, 1, 0),
+                  (8, 4, 2, 0, 0, 0), (4, 4, 2, 3, 0, 0), (8, 4, 2, 3, 1, 0), (16, 3, 2, 0, 1, 0),
+                  (16, 3, 2, 3, 1, 0), (16, 3, 2, 2, 0, 0), (16, 3, 2, 0, 1, 1), (16, 3, 2, 1, 1, 1),
+                  (8, 3, 1, 3, 0, 1)]
+        for shape in shapes:
+            p.set_tuning(*shape)
             c = torch.zeros_like(a)
             p.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), count)
             torch.cuda.synchronize()
             if ref is None:
                 ref = c.clone()
-            assert torch.equal(c, ref), (radix, conv, crt, group, persistent)
+            assert torch.equal(c, ref), shape
         chosen = p.autotune()
         assert chosen["row_radix"] in (4, 8, 16) and chosen["us_per_product"] > 0
         c = torch.zeros_like(a)
@@ -246,7 +248,7 @@ def test_tuning_limits_and_large_default_groups(cuda):
     n, count = 1024, 131
     with make_plan("tensor", n, q, 14) as p:
         for bad in [dict(row_radix=32), dict(group=257), dict(conv_ctas_per_sm=0), dict(crt_ctas_per_sm=5),
-                    dict(row_persistent=2)]:
+                    dict(row_persistent=2), dict(conv_whole_basis=2)]:
             with pytest.raises(polymul.PolymulError):
                 p.set_tuning(**bad)
         p.set_tuning(group=256)
