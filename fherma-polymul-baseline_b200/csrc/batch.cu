@@ -289,6 +289,7 @@ struct BatchCore {
             d.ws_off = ws_off[z];
             d.scale = p->d_scale;
             d.consts = p->d_consts;
+            d.ktab = p->d_ktab;
             d.crt_w = p->d_crt_weights;
             plans.push_back(std::move(p));
         }

@@ -487,14 +487,33 @@ __device__ __forceinline__ void reduce_special(uint32_t (&v)[W + 2], const uint3
 enum CrtReduction { kReduceGeneral = 0, kReduceSpecial = 1, kReduceEither = 2 };
 
 // Final CRT step shared by the SIMT and tensor paths: v += nearest *
-// (-P mod q), reduce mod q, store one coefficient (stride words).
+// (-P mod q), reduce mod q, store one coefficient (stride words).  With ktab
+// (rows k = 0 .. 2P of k (-P mod q) mod q, W words each, 16-byte aligned) the
+// correction is one table row added instead of a W-word multiply-accumulate:
+// the same value mod q, and below v + q, inside reduce_mod_q's range.
 template <int W, int RED = kReduceEither>
 __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t nearest, const uint32_t* s_q,
-                                           uint64_t mu_q, int sbits, uint32_t delta, uint32_t* dst, int stride) {
-    uint32_t pneg[W];
+                                           uint64_t mu_q, int sbits, uint32_t delta, uint32_t* dst, int stride,
+                                           const uint32_t* __restrict__ ktab = nullptr) {
+    if (ktab) {
+        uint32_t row[W + 2];
+        const uint4* r4 = reinterpret_cast<const uint4*>(ktab + size_t(nearest) * W);
 #pragma unroll
-    for (int k = 0; k < W; ++k) pneg[k] = s_q[W + k];
-    crt_mac<W>(v, nearest, pneg);
+        for (int k = 0; k < W / 4; ++k) {
+            const uint4 x = __ldg(r4 + k);
+            row[4 * k] = x.x;
+            row[4 * k + 1] = x.y;
+            row[4 * k + 2] = x.z;
+            row[4 * k + 3] = x.w;
+        }
+        row[W] = row[W + 1] = 0;
+        mp_add<W + 2>(v, row);
+    } else {
+        uint32_t pneg[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) pneg[k] = s_q[W + k];
+        crt_mac<W>(v, nearest, pneg);
+    }
     if constexpr (RED == kReduceSpecial) {
         reduce_special<W>(v, s_q, sbits, delta);
     } else if constexpr (RED == kReduceGeneral) {
@@ -530,7 +549,8 @@ __global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ 
                                                    const PrimeConst* __restrict__ pcs,
                                                    const uint2* __restrict__ tw_inv, const uint2* __restrict__ scale,
                                                    const uint32_t* __restrict__ mq,
-                                                   const uint32_t* __restrict__ consts, uint64_t mu_q, int sbits,
+                                                   const uint32_t* __restrict__ consts,
+                                                   const uint32_t* __restrict__ ktab, uint64_t mu_q, int sbits,
                                                    uint32_t delta, int n, int logR, int logC, int P, int stride,
                                                    size_t io_bstride,
                                                    size_t ws_bstride) {
@@ -586,7 +606,7 @@ __global__ void __launch_bounds__(256) k3_cols_crt(const uint32_t* __restrict__ 
     // nearest integer of sum t_i / p_i (the fraction is f1:f0 / 2^64)
     const uint32_t nearest = uint32_t((f1 + (1ull << 31)) >> 32);
     const size_t J = (size_t(r) << logC) + col0 + g;
-    crt_finish<W>(acc, nearest, s_q, mu_q, sbits, delta, out + J * stride, stride);
+    crt_finish<W>(acc, nearest, s_q, mu_q, sbits, delta, out + J * stride, stride, ktab);
 }
 
 }  // namespace pm

@@ -119,6 +119,7 @@ struct PlanCore {
     DeviceBasis* basis = nullptr;
     uint32_t* d_mq = nullptr;      // [P][W] (P_total/p_i) mod q
     uint32_t* d_consts = nullptr;  // q[W], (-P_total mod q)[W]
+    uint32_t* d_ktab = nullptr;    // [2P+1][W] k (-P_total mod q) mod q: the CRT's quotient correction by table
     uint2* d_scale = nullptr;      // [2P] s_i = 2^32 n^-1 (P_total/p_i)^-1 mod p_i, then s_i psi_i^-brev(1)
     uint32_t* d_work = nullptr;    // [2][P][n] residue planes (plan-owned workspace)
     void* d_batch_work = nullptr;  // residue planes for a group of products (pm_multiply_batch)

@@ -260,6 +260,7 @@ PlanCore::~PlanCore() {
     cudaSetDevice(device);
     cudaFree(d_mq);
     cudaFree(d_consts);
+    cudaFree(d_ktab);
     cudaFree(d_scale);
     for (auto& sl : pipe) sl.reset();
     tensor_release(*this);
@@ -337,6 +338,13 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     const Words pneg = padded(compare(pmod, Words{}) == 0 ? Words{} : subtract(q, pmod), W);
     std::copy(qpad.begin(), qpad.end(), consts.begin());
     std::copy(pneg.begin(), pneg.end(), consts.begin() + W);
+    // k (-P mod q) mod q for every nearest quotient k the CRT can meet: k <= sum t_i / p_i + 1/2
+    // with digits t_i < 2 p_i, so k <= 2P
+    std::vector<uint32_t> ktab(size_t(2 * P + 1) * W, 0);
+    for (unsigned k = 1; k <= 2 * P; ++k) {
+        const Words row = padded(mod(multiply_small(pneg, k), q), W);
+        std::copy(row.begin(), row.end(), ktab.begin() + size_t(k) * W);
+    }
     // mu_q = floor(2^(qbits + 62) / q)
     Words quo;
     Words num(((qbits + 62) / 32) + 1, 0);
@@ -364,6 +372,8 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     cuda_check(cudaMalloc(&d_scale, scale.size() * sizeof(uint2)), "allocate CRT scales");
     cuda_check(cudaMemcpy(d_mq, mq.data(), mq.size() * 4, cudaMemcpyHostToDevice), "upload CRT rows");
     cuda_check(cudaMemcpy(d_consts, consts.data(), consts.size() * 4, cudaMemcpyHostToDevice), "upload q");
+    cuda_check(cudaMalloc(&d_ktab, ktab.size() * 4), "allocate CRT correction table");
+    cuda_check(cudaMemcpy(d_ktab, ktab.data(), ktab.size() * 4, cudaMemcpyHostToDevice), "upload CRT correction table");
     cuda_check(cudaMemcpy(d_scale, scale.data(), scale.size() * sizeof(uint2), cudaMemcpyHostToDevice),
                "upload CRT scales");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
@@ -425,7 +435,8 @@ void launch_k3(const PlanCore& s, const uint32_t* work, uint32_t* c, const Batch
         cuda_check(cudaFuncSetAttribute(k3_cols_crt<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                    "raise K3 shared memory");
     k3_cols_crt<W><<<grid, block, smem, st>>>(work, c, s.basis->d_pc, s.basis->d_tw_inv, s.d_scale, s.d_mq,
-                                              s.d_consts, s.mu_q, int(s.qbits), s.delta, int(s.n), int(s.logR),
+                                              s.d_consts, s.d_ktab, s.mu_q, int(s.qbits), s.delta, int(s.n),
+                                              int(s.logR),
                                               int(s.logC),
                                               int(s.P), int(s.stride), bt.io_bstride, bt.ws_bstride);
 }

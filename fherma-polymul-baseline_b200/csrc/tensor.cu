@@ -217,6 +217,7 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     w.io_bstride = size_t(s.n) * s.stride;
     w.scale = s.d_scale;
     w.consts = s.d_consts;
+    w.ktab = s.d_ktab;
     w.crt_w = s.d_crt_weights;
     w.mu_q = s.mu_q;
     w.sbits = int(s.qbits);

@@ -58,6 +58,7 @@ struct CrtTarget {
     uint32_t* out;           // this product's output coefficients
     const uint2* scale;
     const uint32_t* consts;  // q[W], (-P mod q)[W]
+    const uint32_t* ktab;    // [2P+1][W] k (-P mod q) mod q
     const uint8_t* crt_w;    // [2][128][128] pre-swizzled CRT weights
     uint64_t mu_q;
     int sbits, n, logC, P, stride, use_tma;
@@ -73,6 +74,7 @@ struct BatchProduct {
     uint64_t ws_off;  // u32 words from the batch's workspace base to its planes
     const uint2* scale;
     const uint32_t* consts;
+    const uint32_t* ktab;
     const uint8_t* crt_w;
 };
 
@@ -139,6 +141,7 @@ struct PlanCrtWork {
     size_t ws_bstride, io_bstride;
     const uint2* scale;
     const uint32_t* consts;
+    const uint32_t* ktab;
     const uint8_t* crt_w;
     uint64_t mu_q;
     int sbits, n, logC, P, stride, count, use_tma;
@@ -147,8 +150,8 @@ struct PlanCrtWork {
     __device__ int total() const { return count << lg(); }
     __device__ int2 item(int k) const { return make_int2(k >> lg(), k & ((1 << lg()) - 1)); }
     __device__ CrtTarget target(int z) const {
-        return CrtTarget{&map_res, z, work + z * ws_bstride, out + z * io_bstride, scale, consts, crt_w, mu_q,
-                         sbits, n, logC, P, stride, use_tma, delta};
+        return CrtTarget{&map_res, z, work + z * ws_bstride, out + z * io_bstride, scale, consts, ktab, crt_w,
+                         mu_q, sbits, n, logC, P, stride, use_tma, delta};
     }
 };
 
@@ -166,7 +169,7 @@ struct TableCrtWork {
     }
     __device__ CrtTarget target(int z) const {
         const BatchProduct& d = prod[z];
-        return CrtTarget{maps + 3 * z + 2, 0, work + d.ws_off, out + d.io_off, d.scale, d.consts, d.crt_w,
+        return CrtTarget{maps + 3 * z + 2, 0, work + d.ws_off, out + d.io_off, d.scale, d.consts, d.ktab, d.crt_w,
                          d.mu_q, d.sbits, d.n, d.logC, d.P, d.stride, 1, d.delta};
     }
 };
@@ -588,7 +591,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         const int rr = tid / Gc, cc = tid % Gc;
         if (rr < R) {
             const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
-            crt_finish<W, RED>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride);
+            crt_finish<W, RED>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride, t.ktab);
         }
         }
         tc::fence_before();
