@@ -185,19 +185,25 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
             ph_mma ^= 1u;
             tc::fence_after();
             // --- residues of row m for this half's primes: hi 2^16 + lo, hi and lo below 2^31.01 ---
+            // eight primes per wait: two 16-column loads in flight, their primes' constants
+            // read from shared memory before the wait (the wait orders every memory access)
 #pragma unroll
-            for (int q4 = 0; q4 < 8; ++q4) {
-                if (ilo + 4 * q4 >= ihi) break;  // warp-uniform
-                uint32_t d[16];
-                tc::tmem_ld16(taddr + 16 * q4, d);
+            for (int q8 = 0; q8 < 4; ++q8) {
+                if (ilo + 8 * q8 >= ihi) break;  // warp-uniform
+                uint2 pm[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) pm[u] = spm[ilo + 8 * q8 + u];
+                uint32_t d[2][16];
+                tc::tmem_ld16(taddr + 32 * q8, d[0]);
+                tc::tmem_ld16(taddr + 32 * q8 + 16, d[1]);
                 tc::tmem_wait_ld();
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int i = ilo + 4 * q4 + u;
-                    const uint2 pm = spm[i];
-                    const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8);
-                    const uint32_t hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
-                    sT[i * kTW + row] = reduce48_lazy(lo, hi, pm.x, pm.y);  // [0, 3p): butterfly input
+                for (int u = 0; u < 8; ++u) {
+                    const int i = ilo + 8 * q8 + u;
+                    const uint32_t* e = d[u >> 2] + 4 * (u & 3);
+                    const uint32_t lo = e[0] + (e[1] << 8);
+                    const uint32_t hi = e[2] + (e[3] << 8);
+                    sT[i * kTW + row] = reduce48_lazy(lo, hi, pm[u].x, pm[u].y);  // [0, 3p): butterfly input
                 }
             }
             tc::fence_before();

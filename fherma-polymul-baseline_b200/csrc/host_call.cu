@@ -131,6 +131,32 @@ public:
         if (error_) std::rethrow_exception(error_);
     }
 
+    // The same job without the caller: returns at once; finish() waits for it.
+    void start(int pieces, const std::function<void(int)>& f) {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            job_ = &f;
+            pieces_ = pieces;
+            next_.store(0);
+            done_.store(0);
+            error_ = nullptr;
+            generation_.fetch_add(1, std::memory_order_release);
+        }
+        cv_.notify_all();
+        started_ = pieces;
+    }
+    void finish() {
+        const int pieces = started_;
+        started_ = 0;
+        while (done_.load(std::memory_order_acquire) < pieces) _mm_pause();
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            job_ = nullptr;
+        }
+        while (active_.load(std::memory_order_acquire) > 0) _mm_pause();
+        if (error_) std::rethrow_exception(error_);
+    }
+
 private:
     void work(const std::function<void(int)>* f, int pieces) {
         for (int k = next_.fetch_add(1); k < pieces; k = next_.fetch_add(1)) {
@@ -173,11 +199,13 @@ private:
     std::atomic<int> next_{0}, done_{0}, active_{0};
     std::exception_ptr error_;
     bool stop_ = false;
+    int started_ = 0;
 };
 
 namespace {
 constexpr int kInPieces = 8;   // pieces of each input polynomial
 constexpr int kOutPieces = 8;  // pieces of the product
+static_assert(2 * kInPieces <= 64, "one ready flag per input piece");
 
 int pool_threads() {
     const unsigned hw = std::thread::hardware_concurrency();
@@ -221,29 +249,62 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
     uint8_t* stage = static_cast<uint8_t*>(h.h_stage);
     const uint8_t* src[2] = {reinterpret_cast<const uint8_t*>(a), reinterpret_cast<const uint8_t*>(b)};
     const bool pinned[2] = {is_pinned(a), is_pinned(b)};
-    // every input piece: stage it (pageable source), then queue its H2D right away
-    h.pool->run(2 * kInPieces, [&](int k) {
-        const int poly = k / kInPieces;
-        size_t off, len;
-        piece(io, kInPieces, k % kInPieces, &off, &len);
-        if (!len) return;
-        const uint8_t* from = src[poly] + off;
-        if (!pinned[poly]) {
-            host_copy(stage + poly * io + off, from, len);
-            from = stage + poly * io + off;
+    // pinned inputs go straight to the link in one copy each
+    for (int poly = 0; poly < 2; ++poly)
+        if (pinned[poly])
+            cuda_check(cudaMemcpyAsync(dev + poly * io, src[poly], io, cudaMemcpyHostToDevice, h.stream), "copy in");
+    // pageable inputs: the pool's threads stage the pieces (in index order, as they take
+    // them) while this thread queues each piece's H2D as soon as it is staged -- one thread
+    // talks to the runtime, so the copies enter the stream without contending for it
+    const int staged = (pinned[0] ? 0 : 1) + (pinned[1] ? 0 : 1);
+    if (staged) {
+        const int first = pinned[0] ? 1 : 0;
+        const int np = staged * kInPieces;
+        for (int k = 0; k < np; ++k) h.ready[k].store(0, std::memory_order_relaxed);
+        const std::function<void(int)> stage_piece = [&](int k) {
+            const int poly = first + k / kInPieces;
+            size_t off, len;
+            piece(io, kInPieces, k % kInPieces, &off, &len);
+            if (len) host_copy(stage + poly * io + off, src[poly] + off, len);
+            h.ready[k].store(1, std::memory_order_release);
+        };
+        h.pool->start(np, stage_piece);
+        try {
+            for (int k = 0; k < np; ++k) {
+                const int poly = first + k / kInPieces;
+                size_t off, len;
+                piece(io, kInPieces, k % kInPieces, &off, &len);
+                while (!h.ready[k].load(std::memory_order_acquire)) _mm_pause();
+                if (len)
+                    cuda_check(cudaMemcpyAsync(dev + poly * io + off, stage + poly * io + off, len,
+                                               cudaMemcpyHostToDevice, h.stream),
+                               "copy in");
+            }
+        } catch (...) {
+            try {
+                h.pool->finish();
+            } catch (...) {
+            }
+            throw;
         }
-        cuda_check(cudaMemcpyAsync(dev + poly * io + off, from, len, cudaMemcpyHostToDevice, h.stream), "copy in");
-    });
+        h.pool->finish();
+    }
     launch_product(s, reinterpret_cast<const uint64_t*>(dev), reinterpret_cast<const uint64_t*>(dev + io),
                    reinterpret_cast<uint64_t*>(dev + 2 * io), nullptr, h.stream);
     // a pinned output takes the product directly; otherwise it lands in the staging
     h.direct_out = direct_out && is_pinned(direct_out) ? reinterpret_cast<uint8_t*>(direct_out) : nullptr;
     uint8_t* land = h.direct_out ? h.direct_out : stage + 2 * io;
-    for (int k = 0; k < kOutPieces; ++k) {
-        size_t off, len;
-        piece(io, kOutPieces, k, &off, &len);
-        if (len) cuda_check(cudaMemcpyAsync(land + off, dev + 2 * io + off, len, cudaMemcpyDeviceToHost, h.stream), "copy out");
-        cuda_check(cudaEventRecord(h.out_ready[k], h.stream), "output event");
+    if (h.direct_out) {  // nothing to copy out afterwards: one transfer
+        cuda_check(cudaMemcpyAsync(land, dev + 2 * io, io, cudaMemcpyDeviceToHost, h.stream), "copy out");
+    } else {
+        for (int k = 0; k < kOutPieces; ++k) {
+            size_t off, len;
+            piece(io, kOutPieces, k, &off, &len);
+            if (len)
+                cuda_check(cudaMemcpyAsync(land + off, dev + 2 * io + off, len, cudaMemcpyDeviceToHost, h.stream),
+                           "copy out");
+            cuda_check(cudaEventRecord(h.out_ready[k], h.stream), "output event");
+        }
     }
     // the error word rides on the same stream: no second round trip after the product
     cuda_check(cudaMemcpyAsync(stage + 3 * io, s.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, h.stream),

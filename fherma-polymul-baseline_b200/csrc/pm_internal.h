@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -49,6 +50,9 @@ struct DeviceBasis {
 };
 
 DeviceBasis& basis_for_device(int device);
+PrimeConst prime_const(uint32_t p);
+// Psi_rev[k] = psi^brev(k) and psi^-brev(k) (value, Shoup), k < kNMax, psi of order 2 kNMax mod p
+void twiddle_tables(uint32_t p, uint2* fwd, uint2* inv);
 std::vector<uint32_t> make_primes();
 unsigned basis_size(const std::vector<uint32_t>& primes, unsigned n, unsigned qbits);
 
@@ -72,6 +76,7 @@ struct HostCall {
     void* h_stage = nullptr;        // pinned a, b, c and the error word
     std::vector<cudaEvent_t> out_ready;
     std::unique_ptr<CopyPool> pool;
+    std::atomic<uint8_t> ready[64];  // input piece k staged
     bool pending = false;           // between multiply_host_begin and multiply_host_end
     uint8_t* direct_out = nullptr;  // pinned caller output the product lands in directly, or null
     ~HostCall();
@@ -87,7 +92,7 @@ struct Tuning {
     int conv_ctas_per_sm = 3;  // K1T persistent CTAs per SM (up to four fit; three measured fastest)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
     bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)
-    bool conv_whole_basis = true;  // tensor conversion: one pass of a tile over every prime (K1W) or per group (K1T)
+    bool conv_whole_basis = false;  // tensor conversion: one pass of a tile over every prime (K1W) or per group (K1T)
     uint32_t group = 0;        // products per launch group in batches (0: up to ~2 GB of residues, <= 128)
     bool tuned = false;
 };
@@ -101,6 +106,22 @@ struct WideTables {
     uint32_t* d_tw_inv = nullptr; // [n][W] psi^-brev(k) R mod q
     uint32_t qinv = 0;            // -q^-1 mod 2^32
     ~WideTables();
+};
+
+// Tables of the quartic factorization (PM_QUARTIC, quartic.cu): q = B^4 - delta.
+struct QuarticTables {
+    uint32_t bbits = 0;            // B = 2^bbits
+    uint32_t primes[16] = {};
+    PrimeConst* d_pc = nullptr;    // [64] plane 4i + j: prime i
+    uint2* d_tw_fwd = nullptr;     // [64][kNMax] psi_i^brev(k), plane 4i + j: prime i's table
+    uint2* d_tw_inv = nullptr;
+    uint8_t* d_conv = nullptr;     // [4][64 rows][128 B] conversion weights (channel evaluation folded in)
+    uint8_t* d_crt = nullptr;      // [2][160 rows][128 B] CRT weights (components and quotient groups)
+    uint2* d_mix = nullptr;        // [16] iota_i^-1; then [4][16] scale of component m, prime i
+    uint32_t* d_ktab = nullptr;    // [4][33][W] k (-P 2^(bbits m)) mod q
+    int fix_count = 0;             // straddling bytes at the part boundaries
+    int fix_byte[3] = {}, fix_shift[3] = {};
+    ~QuarticTables();
 };
 
 // Everything one (n, q) product needs on the device.
@@ -134,6 +155,14 @@ struct PlanCore {
     uint32_t tensor_k_crt = 0;
 
     std::unique_ptr<WideTables> wide;  // set for PM_WIDE_NTT plans
+    std::unique_ptr<QuarticTables> quartic;  // set for PM_QUARTIC plans
+
+    // Per-plane tables the kernels index by residue plane: the device basis for the RNS
+    // method, the plan's own for the quartic factorization (a plane per prime and channel).
+    const PrimeConst* plane_pc() const;
+    const uint2* plane_fwd() const;
+    const uint2* plane_inv() const;
+    const uint8_t* conv_weights() const;
 
     Tuning tune;
     std::unique_ptr<PipelineSlot> pipe[3];
@@ -189,6 +218,11 @@ void launch_wide(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32
 // tensor-core conversion / CRT (tensor.cu)
 void tensor_init(PlanCore& s);
 void tensor_release(PlanCore& s);
+
+// quartic factorization (quartic.cu)
+void quartic_init(PlanCore& s);
+void launch_quartic(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
+                    uint32_t count, cudaStream_t st);
 void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
                    uint32_t count, cudaStream_t st);
 

@@ -159,6 +159,34 @@ uint32_t root_of_unity(uint32_t p) {
 }
 }  // namespace
 
+PrimeConst prime_const(uint32_t p) {
+    PrimeConst c{};
+    c.p = p;
+    c.two_p = 2 * p;
+    c.mu = uint32_t((uint64_t(1) << 61) / p);
+    uint32_t pinv = p;  // p^-1 mod 2^32 by Newton: p * p = 1 mod 8, each step doubles the bits
+    for (int it = 0; it < 5; ++it) pinv *= 2u - p * pinv;
+    c.pinv = pinv;
+    c.recip = uint64_t(((unsigned __int128)1 << 64) / p);
+    return c;
+}
+
+// Psi_rev[k] = psi^brev(k) and its inverse, with Shoup companions, k < 65536.
+void twiddle_tables(uint32_t p, uint2* fwd, uint2* inv) {
+    std::vector<uint32_t> ppow(kNMax), ipow(kNMax);
+    const uint32_t psi = root_of_unity(p), ipsi = powmod(psi, p - 2, p);
+    ppow[0] = ipow[0] = 1;
+    for (int e = 1; e < kNMax; ++e) {
+        ppow[e] = mulmod(ppow[e - 1], psi, p);
+        ipow[e] = mulmod(ipow[e - 1], ipsi, p);
+    }
+    for (int k = 0; k < kNMax; ++k) {
+        const uint32_t e = bit_reverse(uint32_t(k), kLogNMax);
+        fwd[k] = make_uint2(ppow[e], shoup_of(ppow[e], p));
+        inv[k] = make_uint2(ipow[e], shoup_of(ipow[e], p));
+    }
+}
+
 DeviceBasis::~DeviceBasis() {
     cudaSetDevice(device);
     cudaFree(d_pc);
@@ -180,33 +208,16 @@ DeviceBasis& basis_for_device(int device) {
     std::vector<uint2> fwd(P * kNMax), inv(P * kNMax), pow(P * kPowWords);
     B->inv1.assign(P, 0);
     auto fill = [&](size_t begin, size_t end) {
-        std::vector<uint32_t> ppow(kNMax), ipow(kNMax);
         for (size_t i = begin; i < end; ++i) {
             const uint32_t p = B->primes[i];
-            const uint32_t psi = root_of_unity(p), ipsi = powmod(psi, p - 2, p);
-            ppow[0] = ipow[0] = 1;
-            for (int e = 1; e < kNMax; ++e) {
-                ppow[e] = mulmod(ppow[e - 1], psi, p);
-                ipow[e] = mulmod(ipow[e - 1], ipsi, p);
-            }
-            for (int k = 0; k < kNMax; ++k) {
-                const uint32_t e = bit_reverse(uint32_t(k), kLogNMax);
-                fwd[i * kNMax + k] = make_uint2(ppow[e], shoup_of(ppow[e], p));
-                inv[i * kNMax + k] = make_uint2(ipow[e], shoup_of(ipow[e], p));
-            }
+            twiddle_tables(p, fwd.data() + i * kNMax, inv.data() + i * kNMax);
             uint32_t w = 1;
             const uint32_t base = uint32_t((uint64_t(1) << 32) % p);
             for (int k = 0; k < kPowWords; ++k) {
                 pow[i * kPowWords + k] = make_uint2(w, shoup_of(w, p));
                 w = mulmod(w, base, p);
             }
-            pc[i].p = p;
-            pc[i].two_p = 2 * p;
-            pc[i].mu = uint32_t((uint64_t(1) << 61) / p);
-            uint32_t pinv = p;  // p^-1 mod 2^32 by Newton: p * p = 1 mod 8, each step doubles the bits
-            for (int it = 0; it < 5; ++it) pinv *= 2u - p * pinv;
-            pc[i].pinv = pinv;
-            pc[i].recip = uint64_t(((unsigned __int128)1 << 64) / p);
+            pc[i] = prime_const(p);
             B->inv1[i] = inv[i * kNMax + 1].x;
         }
     };
@@ -456,7 +467,7 @@ void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStr
             const int ctas = int(std::min<int64_t>(total, int64_t(s.sms) * k2p_min_blocks(LOGC)));
             const PlanRowWork w{work, bt.ws_bstride, int(s.n), int(s.logR), int(s.logC), int(s.P), int(bt.count)};
             k2p_rows<LOGC, KP, PlanRowWork><<<ctas, k2p_threads(LOGC, KP), smem, st>>>(
-                w, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv, int(s.logR), s.d_err);
+                w, s.plane_pc(), s.plane_fwd(), s.plane_inv(), int(s.logR), s.d_err);
             return;
         }
     }
@@ -471,7 +482,7 @@ void launch_k2_fixed(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStr
             cuda_check(cudaFuncSetAttribute(k2_rows<LOGC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                        "raise K2 shared memory");
         dim3 grid(R / rows, s.P, bt.count), block(rows * T);
-        k2_rows<LOGC, KP><<<grid, block, smem, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
+        k2_rows<LOGC, KP><<<grid, block, smem, st>>>(work, s.plane_pc(), s.plane_fwd(), s.plane_inv(),
                                                      int(s.n), int(s.logR), int(s.P), bt.ws_bstride);
     }
 }
@@ -501,7 +512,7 @@ void launch_k2(const PlanCore& s, uint32_t* work, const Batch& bt, cudaStream_t 
         default: {
             const int R = 1 << s.logR;
             dim3 grid((R + 31) / 32, s.P, bt.count), block(R < 32 ? R : 32);
-            k2_rows_small<<<grid, block, 0, st>>>(work, s.basis->d_pc, s.basis->d_tw_fwd, s.basis->d_tw_inv,
+            k2_rows_small<<<grid, block, 0, st>>>(work, s.plane_pc(), s.plane_fwd(), s.plane_inv(),
                                                  int(s.n), int(s.logR), int(s.logC), int(s.P), bt.ws_bstride);
         }
     }
@@ -590,6 +601,11 @@ DeviceScope::~DeviceScope() {
     int now = -1;
     if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous) cudaSetDevice(previous);
 }
+
+const PrimeConst* PlanCore::plane_pc() const { return quartic ? quartic->d_pc : basis->d_pc; }
+const uint2* PlanCore::plane_fwd() const { return quartic ? quartic->d_tw_fwd : basis->d_tw_fwd; }
+const uint2* PlanCore::plane_inv() const { return quartic ? quartic->d_tw_inv : basis->d_tw_inv; }
+const uint8_t* PlanCore::conv_weights() const { return quartic ? quartic->d_conv : basis->d_conv_weights; }
 
 // A kernel that gave up a bounded wait records it in the plan's error word.
 void check_device_errors(const PlanCore& s) {

@@ -158,8 +158,8 @@ void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
     w.P = int(s.P);
     w.count = int(count);
     w.pgs = pgs;
-    k1t_convert<LOGR, PlanConvWork><<<ctas, tc::kConvThreads, smem, st>>>(w, s.basis->d_pc, s.basis->d_conv_weights,
-                                                             s.basis->d_tw_fwd, s.d_err);
+    k1t_convert<LOGR, PlanConvWork><<<ctas, tc::kConvThreads, smem, st>>>(w, s.plane_pc(), s.conv_weights(),
+                                                                           s.plane_fwd(), s.d_err);
 }
 
 // the whole basis per tile: two CTAs per SM, contiguous runs of items
@@ -227,7 +227,7 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     w.P = int(s.P);
     w.stride = int(s.stride);
     w.count = int(count);
-    kernel<<<ctas, tc::kCrtThreads, smem, st>>>(w, s.basis->d_pc, s.basis->d_tw_inv, s.d_err);
+    kernel<<<ctas, tc::kCrtThreads, smem, st>>>(w, s.plane_pc(), s.plane_inv(), s.d_err);
 }
 
 template <int LOGR>
