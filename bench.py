@@ -502,6 +502,30 @@ def run_special(args, torch, polymul, tuning):
         plan.close()
     out["identical"] = bool(all((results[0] == results[1]).flatten()))
     out["speedup"] = out["special_form_products_per_s"] / out["general_reduction_products_per_s"]
+    # the reference's quartic factorization (PM_QUARTIC) on the same batch: 16 primes x 4 channels
+    try:
+        quart = polymul.Plan(n, q, coef_limbs=limbs, quartic=True)
+        C = torch.empty_like(A)
+        st = torch.cuda.Stream()
+        for _ in range(max(args.warmup, 1)):
+            quart.multiply_batch(A.data_ptr(), Bv.data_ptr(), C.data_ptr(), B, stream=st.cuda_stream)
+        st.synchronize()
+        polymul.profile_enable(3 * B * args.steps + 16)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            quart.multiply_batch(A.data_ptr(), Bv.data_ptr(), C.data_ptr(), B, stream=st.cuda_stream)
+        e1.record(st)
+        e1.synchronize()
+        prof = polymul.profile_read()
+        polymul.profile_enable(0)
+        out["quartic_products_per_s"] = B * args.steps / (e0.elapsed_time(e1) / 1000.0)
+        out["quartic_us_per_product"] = {k: 1000.0 * v[1] / (B * args.steps) for k, v in prof.items()}
+        out["quartic_identical"] = bool((C[:4].cpu().numpy().view(np.uint64) == results[1]).all())
+        out["quartic_over_general"] = out["quartic_products_per_s"] / out["general_reduction_products_per_s"]
+        quart.close()
+    except polymul.PolymulError as e:
+        out["quartic"] = f"not applicable at n={n}: {e}"
     # the direct wide-modulus NTT (PM_WIDE_NTT) on the same prime, for comparison: 64 products
     Bw = min(B, 64)
     try:

@@ -57,6 +57,13 @@ struct PlanTileWork {
     }
 };
 
+// Bytes a plan adds to each A row before the MMA (the quartic factorization's part
+// boundaries inside a byte): column 112 + t takes byte[byte[t]] >> shift[t].
+struct ByteFix {
+    int count;
+    int byte[3], shift[3];
+};
+
 constexpr int kTW = 136;  // transpose row stride (words): 4 primes of a warp's pairs 8 banks apart
 constexpr size_t k1w_smem_bytes() { return 1024 + 32768 + 32768 + size_t(tc::kMaxPrimes) * kTW * 4; }
 
@@ -65,7 +72,7 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
                                                                     const PrimeConst* __restrict__ pcs,
                                                                     const uint8_t* __restrict__ conv_w,
                                                                     const uint2* __restrict__ tw_fwd,
-                                                                    uint32_t* __restrict__ err) {
+                                                                    uint32_t* __restrict__ err, const ByteFix fix) {
     constexpr int R = 1 << LOGR;
     constexpr int RT = R > 1 ? R - 1 : 1;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -146,6 +153,14 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
             if (kk >= 1) {  // the workers have read the previous tile's accumulator
                 if (!wait(&tmem_empty, ph_empty)) break;
                 ph_empty ^= 1u;
+            }
+            if (fix.count) {  // the plan's extra bytes, written by this warp, seen by the MMA
+                uint8_t* tile = sA + buf * 16384;
+                for (int m = lane; m < tc::kTileM; m += 32)
+                    for (int t = 0; t < fix.count; ++t)
+                        tile[tc::sw128_offset(m, 112 + t)] = uint8_t(tile[tc::sw128_offset(m, fix.byte[t])] >> fix.shift[t]);
+                tc::fence_smem_async();
+                __syncwarp();
             }
             tc::fence_after();
             if (lane == 0) {

@@ -144,6 +144,21 @@ public:
         }
         cv_.notify_all();
         started_ = pieces;
+        job_started_ = &f;
+    }
+    // The caller takes one piece of the started job, if one is left; false when none is.
+    bool help() {
+        const int pieces = started_;
+        const int k = next_.fetch_add(1);
+        if (k >= pieces) return false;
+        try {
+            (*job_started_)(k);
+        } catch (...) {
+            std::lock_guard<std::mutex> lock(m_);
+            if (!error_) error_ = std::current_exception();
+        }
+        done_.fetch_add(1, std::memory_order_release);
+        return true;
     }
     void finish() {
         const int pieces = started_;
@@ -172,8 +187,9 @@ private:
     void loop() {
         uint64_t seen = 0;
         while (true) {
-            // a short spin catches the next call of a caller that multiplies in a loop
-            const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(200);
+            // spinning a while keeps the threads awake from one half of a product to the next
+            // (the GPU's part lasts a few hundred microseconds) and between back-to-back calls
+            const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(2000);
             while (generation_.load(std::memory_order_acquire) == seen && std::chrono::steady_clock::now() < spin_until)
                 _mm_pause();
             std::unique_lock<std::mutex> lock(m_);
@@ -200,12 +216,13 @@ private:
     std::exception_ptr error_;
     bool stop_ = false;
     int started_ = 0;
+    const std::function<void(int)>* job_started_ = nullptr;
 };
 
 namespace {
 constexpr int kInPieces = 8;   // pieces of each input polynomial
-constexpr int kOutPieces = 8;  // pieces of the product
-static_assert(2 * kInPieces <= 64, "one ready flag per input piece");
+constexpr int kOutPieces = 16;  // pieces of the product
+static_assert(2 * kInPieces <= 64 && kOutPieces <= 64, "one ready flag per piece");
 
 int pool_threads() {
     const unsigned hw = std::thread::hardware_concurrency();
@@ -274,7 +291,9 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
                 const int poly = first + k / kInPieces;
                 size_t off, len;
                 piece(io, kInPieces, k % kInPieces, &off, &len);
-                while (!h.ready[k].load(std::memory_order_acquire)) _mm_pause();
+                // stage pieces too while the next one to queue is not ready (the workers may be waking)
+                while (!h.ready[k].load(std::memory_order_acquire))
+                    if (!h.pool->help()) _mm_pause();
                 if (len)
                     cuda_check(cudaMemcpyAsync(dev + poly * io + off, stage + poly * io + off, len,
                                                cudaMemcpyHostToDevice, h.stream),
@@ -321,14 +340,42 @@ void multiply_host_end(PlanCore& s, uint64_t* c) {
     uint8_t* dst = reinterpret_cast<uint8_t*>(c);
     if (h.direct_out && h.direct_out != dst)
         throw Failure(PM_ERR_INVALID, "the product was directed to another output buffer at the start of the call");
-    // each product piece leaves the staging as soon as it has landed
-    if (!h.direct_out)
-        h.pool->run(kOutPieces, [&](int k) {
+    // each product piece leaves the staging as soon as it has landed: this thread polls the
+    // pieces' events in order (a blocking wait can sleep for longer than a piece takes) and
+    // flags them; the pool's threads copy flagged pieces out
+    if (!h.direct_out) {
+        for (int k = 0; k < kOutPieces; ++k) h.ready[k].store(0, std::memory_order_relaxed);
+        const std::function<void(int)> copy_piece = [&](int k) {
             size_t off, len;
             piece(io, kOutPieces, k, &off, &len);
-            cuda_check(cudaEventSynchronize(h.out_ready[k]), "product");
+            while (!h.ready[k].load(std::memory_order_acquire)) _mm_pause();
             if (len) host_copy(dst + off, stage + 2 * io + off, len);
-        });
+        };
+        h.pool->start(kOutPieces, copy_piece);
+        try {
+            const auto give_up = std::chrono::steady_clock::now() + std::chrono::seconds(60);
+            for (int k = 0; k < kOutPieces; ++k) {
+                cudaError_t e;
+                while ((e = cudaEventQuery(h.out_ready[k])) == cudaErrorNotReady) {
+                    if (std::chrono::steady_clock::now() > give_up)
+                        throw Failure(PM_ERR_TIMEOUT, "the product did not come back within 60 s");
+                    _mm_pause();
+                }
+                cuda_check(e, "product");
+                h.ready[k].store(1, std::memory_order_release);
+            }
+        } catch (...) {
+            for (int k = 0; k < kOutPieces; ++k) h.ready[k].store(1, std::memory_order_release);  // release the copiers
+            try {
+                h.pool->finish();
+            } catch (...) {
+            }
+            throw;
+        }
+        while (h.pool->help()) {
+        }
+        h.pool->finish();
+    }
     cuda_check(cudaStreamSynchronize(h.stream), "product");
     uint32_t herr = 0;
     std::memcpy(&herr, stage + 3 * io, sizeof herr);

@@ -288,8 +288,10 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     if (!q64 || q_limbs == 0) throw Failure(PM_ERR_INVALID, "q is missing");
     if (n_ < 2 || (n_ & (n_ - 1))) throw Failure(PM_ERR_INVALID, "n must be a power of two >= 2");
     if (n_ > uint32_t(kNMax)) throw Failure(PM_ERR_UNSUPPORTED, "n above 65536");
-    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_CONVERT_SIMT | PM_SPECIAL_FORM | PM_WIDE_NTT))
+    if (flags_ & ~uint32_t(PM_CONVERT_TENSOR | PM_CONVERT_SIMT | PM_SPECIAL_FORM | PM_WIDE_NTT | PM_QUARTIC))
         throw Failure(PM_ERR_INVALID, "unknown flags");
+    if ((flags_ & PM_QUARTIC) && (flags_ & (PM_CONVERT_SIMT | PM_WIDE_NTT)))
+        throw Failure(PM_ERR_INVALID, "PM_QUARTIC runs on the tensor path only");
     if ((flags_ & PM_CONVERT_TENSOR) && (flags_ & PM_CONVERT_SIMT))
         throw Failure(PM_ERR_INVALID, "PM_CONVERT_TENSOR and PM_CONVERT_SIMT exclude each other");
     // no path asked for: the tensor path wherever its 16-byte coefficient rows exist
@@ -372,6 +374,7 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
         if (bit_length(d) <= 32) delta = d.empty() ? 0u : d[0];
     }
 
+    if (flags & PM_QUARTIC) quartic_init(*this);  // 64 planes (16 primes x 4 channels), its own tables
     workspace_bytes = size_t(2) * P * n * sizeof(uint32_t);
     if (flags & PM_WIDE_NTT) {
         wide_init(*this);
@@ -391,7 +394,7 @@ void PlanCore::init(uint32_t n_, const uint64_t* q64, uint32_t q_limbs, uint32_t
     if (sms <= 0) sms = 148;
     cuda_check(cudaMalloc(&d_err, sizeof(uint32_t)), "allocate error word");
     cuda_check(cudaMemset(d_err, 0, sizeof(uint32_t)), "clear error word");
-    if (flags & PM_CONVERT_TENSOR) tensor_init(*this);
+    if ((flags & PM_CONVERT_TENSOR) && !quartic) tensor_init(*this);
     if (tables_only) return;
     cuda_check(cudaMalloc(&d_work, workspace_bytes), "allocate residue workspace");
     cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "create plan stream");
@@ -645,6 +648,8 @@ void launch_batch(const PlanCore& s, const uint64_t* a, const uint64_t* b, uint6
         uint32_t* c32 = reinterpret_cast<uint32_t*>(c) + z * io_words;
         if (s.wide)
             launch_wide(s, a32, b32, c32, work, g, st);
+        else if (s.quartic)
+            launch_quartic(s, a32, b32, c32, work, g, st);
         else if (s.flags & PM_CONVERT_TENSOR)
             launch_tensor(s, a32, b32, c32, work, g, st);
         else

@@ -15,6 +15,7 @@
 #include "tc_ptx.cuh"
 #include "tensor_kernels.cuh"
 #include "convert_tile.cuh"
+#include "crt_quartic.cuh"
 
 namespace pm {
 
@@ -183,8 +184,16 @@ void launch_k1w(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
     w.logC = int(s.logC);
     w.P = int(s.P);
     w.count = int(count);
-    k1w_convert<LOGR, PlanTileWork><<<ctas, tc::kWideThreads, smem, st>>>(w, s.basis->d_pc, s.basis->d_conv_weights,
-                                                                        s.basis->d_tw_fwd, s.d_err);
+    ByteFix fix{};
+    if (s.quartic) {
+        fix.count = s.quartic->fix_count;
+        for (int t = 0; t < 3; ++t) {
+            fix.byte[t] = s.quartic->fix_byte[t];
+            fix.shift[t] = s.quartic->fix_shift[t];
+        }
+    }
+    k1w_convert<LOGR, PlanTileWork><<<ctas, tc::kWideThreads, smem, st>>>(w, s.plane_pc(), s.conv_weights(),
+                                                                        s.plane_fwd(), s.d_err, fix);
 }
 
 template <int LOGR>
@@ -244,6 +253,68 @@ void launch_k3t_w(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t
     }
 }
 }  // namespace
+
+namespace {
+template <int LOGR, int W>
+void launch_k3q(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t count, cudaStream_t st) {
+    const QuarticTables& Q = *s.quartic;
+    const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
+    if ((C * 4) % 16) throw Failure(PM_ERR_UNSUPPORTED, "quartic plans need n >= 64");
+    const int items = int(count) * (C / Gc);
+    int ctas = s.sms * 2;
+    if (ctas > items) ctas = items;
+    const size_t smem = k3q_smem_bytes<LOGR>();
+    auto kernel = s.delta ? k3q_crt<LOGR, W, kReduceSpecial> : k3q_crt<LOGR, W, kReduceGeneral>;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "K3Q shared memory");
+    QuarticCrtWork w;
+    w.map_res = residue_map(s, work, count);
+    w.out = c;
+    w.io_bstride = size_t(s.n) * s.stride;
+    w.consts = s.d_consts;
+    w.ktab = Q.d_ktab;
+    w.crt_w = Q.d_crt;
+    w.mix = Q.d_mix;
+    w.mu_q = s.mu_q;
+    w.sbits = int(s.qbits);
+    w.delta = s.delta;
+    w.n = int(s.n);
+    w.logC = int(s.logC);
+    w.stride = int(s.stride);
+    w.count = int(count);
+    kernel<<<ctas, tc::kCrtThreads, smem, st>>>(w, s.plane_pc(), s.plane_inv(), s.d_err);
+}
+}  // namespace
+
+// The quartic factorization: K1W with the plan's channel-evaluating weights, the row
+// kernel over its 64 planes, and K3Q.
+void launch_quartic(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
+                    uint32_t count, cudaStream_t st) {
+    {
+        ProfileScope prof("k1t_convert_cols", st);
+        switch (s.logR) {
+            case 4: launch_k1w<4>(s, a, b, work, count, st); break;
+            case 3: launch_k1w<3>(s, a, b, work, count, st); break;
+            case 2: launch_k1w<2>(s, a, b, work, count, st); break;
+            default: throw Failure(PM_ERR_UNSUPPORTED, "quartic plans need n >= 64");
+        }
+    }
+    {
+        ProfileScope prof("k2_rows", st);
+        launch_rows(s, work, count, st);
+    }
+    {
+        ProfileScope prof("k3t_cols_crt", st);
+        if (s.W != 28) throw Failure(PM_ERR_UNSUPPORTED, "quartic plans take q of 865..896 bits");
+        switch (s.logR) {
+            case 4: launch_k3q<4, 28>(s, work, c, count, st); break;
+            case 3: launch_k3q<3, 28>(s, work, c, count, st); break;
+            default: launch_k3q<2, 28>(s, work, c, count, st); break;
+        }
+    }
+    cuda_check(cudaGetLastError(), "launch quartic product kernels");
+    count_launches(3);
+}
 
 void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
                    uint32_t count, cudaStream_t st) {

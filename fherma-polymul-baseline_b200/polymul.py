@@ -30,6 +30,7 @@ PM_CONVERT_TENSOR = 1
 PM_CONVERT_SIMT = 8
 PM_SPECIAL_FORM = 2
 PM_WIDE_NTT = 4
+PM_QUARTIC = 16
 
 _lib = None
 
@@ -164,7 +165,7 @@ def selftest_bounded_wait(limit_us):
 class Plan:
     """A product plan for (n, q): basis, CRT constants, workspace, staging."""
 
-    def __init__(self, n, q, coef_limbs=None, tensor=None, special_form=False, wide=False):
+    def __init__(self, n, q, coef_limbs=None, tensor=None, special_form=False, wide=False, quartic=False):
         """tensor: None lets the library choose (the tensor path when coef_limbs is even),
         True asks for the tcgen05 conversion/CRT, False for the plain method."""
         self.q = int(q)
@@ -175,7 +176,8 @@ class Plan:
         check(lib().pm_plan_create(ctypes.byref(self._h), self.n,
                                    qarr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(qarr),
                                    self.coef_limbs, self._convert_flag(tensor)
-                                   | (PM_SPECIAL_FORM if special_form else 0) | (PM_WIDE_NTT if wide else 0)))
+                                   | (PM_SPECIAL_FORM if special_form else 0) | (PM_WIDE_NTT if wide else 0)
+                                   | (PM_QUARTIC if quartic else 0)))
         info = PlanInfo()
         check(lib().pm_plan_get_info(self._h, ctypes.byref(info)))
         self.info = info

@@ -57,7 +57,16 @@ enum pm_flags {
      * each butterfly a W-word Montgomery multiplication, no residues and no CRT.  Needs a
      * prime q = 1 (mod 2n) (the FHERMA modulus 2^868 - 11993087 is one at n <= 32768);
      * PM_ERR_UNSUPPORTED otherwise.  Same results as the RNS method, several times slower. */
-    PM_WIDE_NTT = 4
+    PM_WIDE_NTT = 4,
+    /* The reference's quartic factorization (its best backend, quartic/host_setup.h:41-110,
+     * quartic/solve.cu) for q = B^4 - delta with B = 2^(bits(q)/4), 0 < delta < 2^28, q of
+     * 772..896 bits, a multiple of 4 (the FHERMA modulus 2^868 - 11993087 is one): each coefficient split in
+     * four parts of bits(q)/4 bits, the product taken in Z[X, Y] / (X^n + 1, Y^4 - delta)
+     * modulo 16 primes in which delta is a fourth power, each at the four roots of
+     * Y^4 = delta (64 residue planes), then interpolated and recombined with
+     * Y = B mod q.  Tensor path only, coef_limbs = 14, 64 <= n; PM_ERR_UNSUPPORTED when
+     * 16 primes below 2^30 do not cover n (1 + 3 delta) B^2 four times over. */
+    PM_QUARTIC = 16
 };
 
 typedef struct {
