@@ -157,8 +157,11 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
             if (fix.count) {  // the plan's extra bytes, written by this warp, seen by the MMA
                 uint8_t* tile = sA + buf * 16384;
                 for (int m = lane; m < tc::kTileM; m += 32)
-                    for (int t = 0; t < fix.count; ++t)
-                        tile[tc::sw128_offset(m, 112 + t)] = uint8_t(tile[tc::sw128_offset(m, fix.byte[t])] >> fix.shift[t]);
+#pragma unroll
+                    for (int t = 0; t < 3; ++t)  // constant indices: the parameter stays out of local memory
+                        if (t < fix.count)
+                            tile[tc::sw128_offset(m, 112 + t)] =
+                                uint8_t(tile[tc::sw128_offset(m, fix.byte[t])] >> fix.shift[t]);
                 tc::fence_smem_async();
                 __syncwarp();
             }

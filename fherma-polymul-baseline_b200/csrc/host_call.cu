@@ -223,10 +223,10 @@ namespace {
 // Every copy the link makes costs about 3.7 us of its time on top of the bytes (B200,
 // PCIe 5: 7.3 MB in 16 copies took 196 us against 139 us in one), so the host threads
 // work in small units while the link gets few large copies:
-constexpr int kInUnits = 16;   // staging units of each input polynomial
+constexpr int kInUnits = 18;   // staging units of each input polynomial (9 per copy: one round of the threads)
 constexpr int kInCopies = 2;   // H2D copies of each input polynomial (kInUnits / kInCopies units each)
 constexpr int kOutPieces = 4;  // D2H copies of the product
-constexpr int kOutUnits = 16;  // copy-out units of the product (kOutUnits / kOutPieces per copy)
+constexpr int kOutUnits = 36;  // copy-out units of the product (9 per copy)
 static_assert(kInUnits % kInCopies == 0 && kOutUnits % kOutPieces == 0, "whole units per copy");
 static_assert(2 * kInUnits <= 64 && kOutPieces <= 64, "one ready flag per unit");
 

@@ -26,6 +26,7 @@
 #include <cuda.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "pm_device.cuh"
 #include "tc_ptx.cuh"
@@ -437,6 +438,8 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
     __shared__ uint64_t tma_bar, mma_bar;
     __shared__ uint32_t tmem_base;
     __shared__ uint32_t s_q[2 * W];
+    __shared__ uint32_t s_p[tc::kMaxPrimes];                // the product's primes
+    __shared__ uint2 s_sc[2 * tc::kMaxPrimes];              // its CRT scales s_i, then s_i psi_i^-brev(1)
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int total = w.total();
@@ -480,6 +483,11 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             const uint4* src = reinterpret_cast<const uint4*>(t.crt_w);
             for (int q = tid; q < 2048; q += tc::kCrtThreads) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
             for (int q = tid; q < 2 * W; q += tc::kCrtThreads) s_q[q] = t.consts[q];
+            for (int q = tid; q < t.P; q += tc::kCrtThreads) {
+                s_p[q] = __ldg(&pcs[q].p);
+                s_sc[q] = __ldg(t.scale + q);
+                s_sc[tc::kMaxPrimes + q] = __ldg(t.scale + t.P + q);
+            }
             if (R > 1)
                 for (int q = tid; q < t.P * RT; q += tc::kCrtThreads)
                     sTw[q] = __ldg(tw_inv + size_t(q / RT) * kNMax + 1 + q % RT);
@@ -503,12 +511,16 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         }
         // --- inverse column stages and CRT digits into A ---
         const int pairs = t.P * Gc;
-        for (int pr = tid; pr < pairs; pr += tc::kCrtThreads) {
-            const int i = pr / Gc, c = pr - i * Gc;
-            const uint32_t p = __ldg(&pcs[i].p), two_p = 2 * p;
+        // one (prime, column) pair; G is the tile's column count when known at compile time
+        auto digits = [&](auto gconst, int pr) {
+            constexpr int G = decltype(gconst)::value;
+            const int gc = G ? G : Gc;
+            const int i = G ? pr / G : pr / Gc, c = pr - i * gc;
+            const int P = t.P;
+            const uint32_t p = s_p[i], two_p = 2 * p;
             uint32_t v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = sR[(r * t.P + i) * Gc + c];
+            for (int r = 0; r < R; ++r) v[r] = sR[(r * P + i) * gc + c];
             const uint2* tw = sTw + i * RT - 1;  // tw[k] = Psi_inv_rev[k], k >= 1
 #pragma unroll
             for (int s = LOGR - 1; s >= 1; --s) {
@@ -520,9 +532,9 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             // last stage (one twiddle per prime) with the CRT scale s_i folded in:
             // x' = s_i (x + y), y' = s_i w (x - y); digits t_i in [0, 2p) (an extra p_i
             // adds P to the CRT sum and 1 to its nearest quotient, which cancel)
-            const uint2 sc = __ldg(t.scale + i);
+            const uint2 sc = s_sc[i];
             if constexpr (LOGR > 0) {
-                const uint2 sw = __ldg(t.scale + t.P + i);
+                const uint2 sw = s_sc[tc::kMaxPrimes + i];
 #pragma unroll
                 for (int r = 0; r < R / 2; ++r) {
                     const uint32_t x = v[r], y = v[r + R / 2];
@@ -535,7 +547,12 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             const uint32_t ka = uint32_t(i) >> 5, kb = (4u * i) & 127u;
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(r * Gc + c, kb)) = v[r];
+                *reinterpret_cast<uint32_t*>(sA + ka * 16384 + tc::sw128_offset(r * gc + c, kb)) = v[r];
+        };
+        if (Gc == 8) {
+            for (int pr = tid; pr < pairs; pr += tc::kCrtThreads) digits(std::integral_constant<int, 8>{}, pr);
+        } else {
+            for (int pr = tid; pr < pairs; pr += tc::kCrtThreads) digits(std::integral_constant<int, 0>{}, pr);
         }
         tc::fence_smem_async();
         tc::fence_before();
