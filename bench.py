@@ -943,10 +943,16 @@ def run_ours(args):
         mhz = clocks.get("sm_mhz") or 1965.0
         peak_bfly = 128.0 / 7.0 * sms * mhz * 1e6
         achieved = bfly * timed_products / (tot / 1000.0)
+        # the integer multiplier (fmaheavy pipe) bound: a butterfly's three multiplies hold it
+        # 2 + 4 (the high product) + 2 cycles per warp, one pipe per SM sub-partition
+        peak_mul = 32.0 / 8.0 * 4 * sms * mhz * 1e6
         alu = {"kernel": "k2_rows", "butterflies_per_product": bfly, "achieved_per_s": achieved,
                "peak_per_s": peak_bfly, "frac": achieved / peak_bfly,
                "unit": "butterflies/s", "sm_mhz": mhz,
-               "model": "issue bound: 7 thread instructions per lazy butterfly, 128 per SM per clock"}
+               "model": "issue bound: 7 thread instructions per lazy butterfly, 128 per SM per clock",
+               "multiplier_bound": {"peak_per_s": peak_mul, "frac": achieved / peak_mul,
+                                    "model": "fmaheavy pipe: 8 cycles per warp-butterfly (IMAD 2 + IMAD.HI 4 + "
+                                             "IMAD 2), 4 sub-partitions per SM"}}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
