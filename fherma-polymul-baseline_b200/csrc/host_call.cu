@@ -23,6 +23,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <immintrin.h>
@@ -85,6 +86,21 @@ bool is_pinned(const void* p) {
 }
 
 }  // namespace
+
+// How long an idle copy thread spins before it sleeps: PM_HOST_SPIN_US (microseconds,
+// read once), 2000 by default.  A caller that leaves longer gaps between products (a
+// harness reading its next case from disk) finds the threads asleep and waits for them
+// to wake; a longer spin trades host CPU time for that latency.
+static long spin_us() {
+    static const long us = [] {
+        const char* e = std::getenv("PM_HOST_SPIN_US");
+        if (!e || !*e) return 2000L;
+        char* end = nullptr;
+        const long v = std::strtol(e, &end, 10);
+        return (end && *end == 0 && v >= 0 && v <= 10000000L) ? v : 2000L;
+    }();
+    return us;
+}
 
 // Persistent host threads that run the pieces of one job; the calling thread
 // takes pieces too.  Idle workers spin for a short while (back-to-back calls
@@ -189,7 +205,7 @@ private:
         while (true) {
             // spinning a while keeps the threads awake from one half of a product to the next
             // (the GPU's part lasts a few hundred microseconds) and between back-to-back calls
-            const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(2000);
+            const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(spin_us());
             while (generation_.load(std::memory_order_acquire) == seen && std::chrono::steady_clock::now() < spin_until)
                 _mm_pause();
             std::unique_lock<std::mutex> lock(m_);
@@ -222,13 +238,63 @@ private:
 namespace {
 // Every copy the link makes costs about 3.7 us of its time on top of the bytes (B200,
 // PCIe 5: 7.3 MB in 16 copies took 196 us against 139 us in one), so the host threads
-// work in small units while the link gets few large copies:
-constexpr int kInUnits = 18;   // staging units of each input polynomial (9 per copy: one round of the threads)
-constexpr int kInCopies = 2;   // H2D copies of each input polynomial (kInUnits / kInCopies units each)
-constexpr int kOutPieces = 4;  // D2H copies of the product
-constexpr int kOutUnits = 36;  // copy-out units of the product (9 per copy)
-static_assert(kInUnits % kInCopies == 0 && kOutUnits % kOutPieces == 0, "whole units per copy");
-static_assert(2 * kInUnits <= 64 && kOutPieces <= 64, "one ready flag per unit");
+// work in small units while the link gets few copies.  A staged input goes in copy
+// groups of kGroupUnits units (one round of the threads); the first polynomial's groups
+// grow geometrically (1/16, 1/8, 1/4, then the remaining 9/16) so that the link starts
+// after a small first round instead of a quarter of the bytes -- the threads stage about
+// twice as fast as the link moves -- and the second polynomial, staged while the first is
+// on the link, goes in two halves.
+constexpr int kGroupUnits = 9;  // staging units per H2D copy
+constexpr int kMaxGroups = 6;   // H2D copies of the staged inputs (4 + 2)
+constexpr int kOutPieces = 4;   // D2H copies of the product: 1/2, 1/4, 1/8, 1/8 of it, the last
+                                // one's copy-out (after everything else) short
+static_assert(kMaxGroups * kGroupUnits <= 64 && kOutPieces <= 64, "one ready flag per unit");
+
+// D2H piece k of the product: offset and length
+void out_piece(size_t io, int k, size_t* off, size_t* len) {
+    const auto cut = [](size_t x) { return x & ~size_t(63); };
+    const size_t b1 = cut(io / 2), b2 = b1 + cut(io / 4), b3 = b2 + cut(io / 8);
+    const size_t bound[kOutPieces + 1] = {0, b1, b2, b3, io};
+    *off = bound[k];
+    *len = bound[k + 1] - bound[k];
+}
+
+// the H2D copies of the staged inputs: polynomial, byte offset and length of each
+struct InGroups {
+    int count = 0;
+    int poly[kMaxGroups];
+    size_t off[kMaxGroups], len[kMaxGroups];
+    void add(int p, size_t o, size_t l) {
+        poly[count] = p;
+        off[count] = o;
+        len[count] = l;
+        ++count;
+    }
+};
+
+InGroups input_groups(size_t io, bool pinned_a, bool pinned_b) {
+    InGroups g;
+    const auto cut = [](size_t x) { return x & ~size_t(63); };
+    bool first = true;
+    for (int poly = 0; poly < 2; ++poly) {
+        if (poly == 0 ? pinned_a : pinned_b) continue;
+        if (first) {
+            size_t o = 0;
+            for (int d = 16; d >= 4; d /= 2) {
+                const size_t l = std::min(io - o, cut(io / size_t(d)));
+                if (l) g.add(poly, o, l);
+                o += l;
+            }
+            if (io > o) g.add(poly, o, io - o);
+            first = false;
+        } else {
+            const size_t h = std::min(io, cut(io / 2 + 63));
+            g.add(poly, 0, h);
+            if (io > h) g.add(poly, h, io - h);
+        }
+    }
+    return g;
+}
 
 int pool_threads() {
     const unsigned hw = std::thread::hardware_concurrency();
@@ -277,37 +343,32 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
         if (pinned[poly])
             cuda_check(cudaMemcpyAsync(dev + poly * io, src[poly], io, cudaMemcpyHostToDevice, h.stream), "copy in");
     // pageable inputs: the pool's threads stage the units (in index order, as they take
-    // them) while this thread queues a polynomial's copies as soon as their units are staged
-    // -- one thread talks to the runtime, so the copies enter the stream without contending
-    const int staged = (pinned[0] ? 0 : 1) + (pinned[1] ? 0 : 1);
-    if (staged) {
-        const int first = pinned[0] ? 1 : 0;
-        const int nu = staged * kInUnits;
+    // them) while this thread queues each copy group as soon as its units are staged -- one
+    // thread talks to the runtime, so the copies enter the stream without contending
+    const InGroups g = input_groups(io, pinned[0], pinned[1]);
+    if (g.count) {
+        const int nu = g.count * kGroupUnits;
         for (int k = 0; k < nu; ++k) h.ready[k].store(0, std::memory_order_relaxed);
         const std::function<void(int)> stage_unit = [&](int k) {
-            const int poly = first + k / kInUnits;
+            const int grp = k / kGroupUnits, poly = g.poly[grp];
             size_t off, len;
-            piece(io, kInUnits, k % kInUnits, &off, &len);
+            piece(g.len[grp], kGroupUnits, k % kGroupUnits, &off, &len);
+            off += g.off[grp];
             if (len) host_copy(stage + poly * io + off, src[poly] + off, len);
             h.ready[k].store(1, std::memory_order_release);
         };
         h.pool->start(nu, stage_unit);
         try {
-            constexpr int per = kInUnits / kInCopies;
-            for (int g = 0; g < staged * kInCopies; ++g) {
-                const int poly = first + g / kInCopies, u0 = (g % kInCopies) * per;
+            for (int grp = 0; grp < g.count; ++grp) {
                 // stage units too while this copy's are not all ready (the workers may be waking)
-                for (int k = g * per; k < (g + 1) * per; ++k)
+                for (int k = grp * kGroupUnits; k < (grp + 1) * kGroupUnits; ++k)
                     while (!h.ready[k].load(std::memory_order_acquire))
                         if (!h.pool->help()) _mm_pause();
-                size_t off0, len0, off1, len1;
-                piece(io, kInUnits, u0, &off0, &len0);
-                piece(io, kInUnits, u0 + per - 1, &off1, &len1);
-                const size_t len = off1 + len1 - off0;
-                if (len)
-                    cuda_check(cudaMemcpyAsync(dev + poly * io + off0, stage + poly * io + off0, len,
-                                               cudaMemcpyHostToDevice, h.stream),
-                               "copy in");
+                const size_t off = g.off[grp];
+                uint8_t* dst = dev + g.poly[grp] * io + off;
+                cuda_check(cudaMemcpyAsync(dst, stage + g.poly[grp] * io + off, g.len[grp], cudaMemcpyHostToDevice,
+                                           h.stream),
+                           "copy in");
             }
         } catch (...) {
             try {
@@ -328,7 +389,7 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
     } else {
         for (int k = 0; k < kOutPieces; ++k) {
             size_t off, len;
-            piece(io, kOutPieces, k, &off, &len);
+            out_piece(io, k, &off, &len);
             if (len)
                 cuda_check(cudaMemcpyAsync(land + off, dev + 2 * io + off, len, cudaMemcpyDeviceToHost, h.stream),
                            "copy out");
@@ -355,18 +416,16 @@ void multiply_host_end(PlanCore& s, uint64_t* c) {
     // flags them; the pool's threads copy the units of flagged pieces out
     if (!h.direct_out) {
         for (int k = 0; k < kOutPieces; ++k) h.ready[k].store(0, std::memory_order_relaxed);
-        size_t p0, plen;
-        piece(io, kOutPieces, 0, &p0, &plen);  // D2H piece size (the last may be shorter)
-        const std::function<void(int)> copy_unit = [&](int k) {
-            size_t off, len;
-            piece(io, kOutUnits, k, &off, &len);
+        const std::function<void(int)> copy_unit = [&](int k) {  // unit k % 9 of piece k / 9
+            const int pc = k / kGroupUnits;
+            size_t poff, plen, off, len;
+            out_piece(io, pc, &poff, &plen);
+            piece(plen, kGroupUnits, k % kGroupUnits, &off, &len);
             if (!len) return;
-            // the copies land in order: the piece holding the unit's last byte brings all of it
-            const size_t last = (off + len - 1) / plen;
-            while (!h.ready[last].load(std::memory_order_acquire)) _mm_pause();
-            host_copy(dst + off, stage + 2 * io + off, len);
+            while (!h.ready[pc].load(std::memory_order_acquire)) _mm_pause();
+            host_copy(dst + poff + off, stage + 2 * io + poff + off, len);
         };
-        h.pool->start(kOutUnits, copy_unit);
+        h.pool->start(kOutPieces * kGroupUnits, copy_unit);
         try {
             const auto give_up = std::chrono::steady_clock::now() + std::chrono::seconds(60);
             for (int k = 0; k < kOutPieces; ++k) {

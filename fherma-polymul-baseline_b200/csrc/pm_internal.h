@@ -92,7 +92,7 @@ struct Tuning {
     int conv_ctas_per_sm = 3;  // K1T persistent CTAs per SM (up to four fit; three measured fastest)
     int crt_ctas_per_sm = 2;   // K3T persistent CTAs per SM
     bool row_persistent = true;  // K2 as the persistent, prefetching kernel (rows of C >= 1024)
-    bool conv_whole_basis = false;  // tensor conversion: one pass of a tile over every prime (K1W) or per group (K1T)
+    bool conv_whole_basis = true;  // tensor conversion: one pass of a tile over every prime (K1W) or per group (K1T)
     uint32_t group = 0;        // products per launch group in batches (0: up to ~2 GB of residues, <= 128)
     bool tuned = false;
 };

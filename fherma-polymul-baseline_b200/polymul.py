@@ -247,7 +247,7 @@ class Plan:
         return {name: getattr(t, name) for name, _ in Tuning._fields_}
 
     def set_tuning(self, row_radix=16, conv_ctas_per_sm=3, crt_ctas_per_sm=2, group=0, row_persistent=1,
-                   conv_whole_basis=0):
+                   conv_whole_basis=1):
         t = Tuning(row_radix, conv_ctas_per_sm, crt_ctas_per_sm, group, row_persistent, conv_whole_basis, 0.0)
         check(lib().pm_plan_set_tuning(self._h, ctypes.byref(t)))
 

@@ -101,9 +101,9 @@ typedef struct {
                                    128 products; at most 256) */
     uint32_t row_persistent;    /* 1: rows of >= 1024 values by the persistent kernel that stages a row's
                                    twiddles once per group and prefetches rows; 0: one CTA per row */
-    uint32_t conv_whole_basis;  /* tensor conversion: 1 takes each coefficient tile through all primes at once
-                                   (weights of the whole basis resident, 2 CTAs per SM; conv_ctas_per_sm
-                                   unused); 0 runs it once per group of 16 primes */
+    uint32_t conv_whole_basis;  /* tensor conversion: 1 (the default) takes each coefficient tile through all
+                                   primes at once (weights of the whole basis resident, 2 CTAs per SM;
+                                   conv_ctas_per_sm unused); 0 runs it once per group of 16 primes */
     double us_per_product;      /* device time the autotuner measured (-1: taken from its cache) */
 } pm_tuning;
 
