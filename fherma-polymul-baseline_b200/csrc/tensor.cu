@@ -59,7 +59,10 @@ void tensor_init(PlanCore& s) {
                        "upload conversion weights");
         }
     }
-    // CRT weights: [2 K-atoms][128 rows][128 B]
+    // CRT weights: [2 K-atoms][128 rows][128 B].  Row (i, a) holds the bytes of
+    // ((P/p_i) mod q) 2^(8a) mod q: digit byte a of t_i times it sums, over a, to
+    // t_i (P/p_i) mod q, and the whole contraction stays below 4P 255 q < 2^16 q,
+    // so the CRT's final reduction removes a one-word quotient.
     const uint32_t NV = 4 * s.W + 4;
     Words total{1};
     for (unsigned i = 0; i < s.P; ++i) total = multiply_small(total, B.primes[i]);
@@ -70,7 +73,7 @@ void tensor_init(PlanCore& s) {
         const Words mq = mod(m, s.q);
         const uint64_t recip = uint64_t(((unsigned __int128)1 << 64) / B.primes[i]);
         for (int a = 0; a < 4; ++a) {
-            const Words shifted = shift_left(mq, 8 * a);
+            const Words shifted = mod(shift_left(mq, 8 * a), s.q);
             const unsigned __int128 rs = (unsigned __int128)recip << (8 * a);
             const uint32_t k = 4 * i + a, ka = k >> 7, kk = k & 127;
             for (uint32_t J = 0; J < NV; ++J) {

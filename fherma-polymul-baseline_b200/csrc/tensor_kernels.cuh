@@ -406,6 +406,28 @@ __global__ void __launch_bounds__(tc::kConvThreads, 4) k1t_convert(const __grid_
     if (!ok) atomicOr(err, 1u);
 }
 
+// a[0..3] += b[0..3] + cy, cy in {0, 1} in and out (one add-with-carry chain;
+// adding 2^32 - 1 to cy sets the carry flag exactly when cy is 1)
+__device__ __forceinline__ void add4_carry(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3,
+                                           const uint32_t (&b)[4], uint32_t& cy) {
+    asm("add.cc.u32 %4, %4, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32 %4, 0, 0;"
+        : "+r"(a0), "+r"(a1), "+r"(a2), "+r"(a3), "+r"(cy)
+        : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]));
+}
+__device__ __forceinline__ void add1_carry(uint32_t& a, uint32_t b, uint32_t& cy) {
+    asm("add.cc.u32 %1, %1, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 %0, %0, %2;\n\t"
+        "addc.u32 %1, 0, 0;"
+        : "+r"(a), "+r"(cy)
+        : "r"(b));
+}
+
+// ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
 // K3T: inverse column stages + CRT on the tensor cores, persistent.  Block of
 // kCrtThreads = 256: all eight warps run the digit phase (the column stages of
@@ -573,43 +595,70 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         ok = tc::mbar_wait(&mma_bar, mma_phase) && ok;
         mma_phase ^= 1;
         tc::fence_after();
-        // --- carry-propagate the byte columns of row m = tid (warps 0-3, the TMEM lane owners) ---
-        // value: NV/4 = W+1 words plus the carry-out; quotient estimate: 8 columns
+        // --- the CRT value of row m = tid (warps 0-3, the TMEM lane owners) ---
+        // Word j of the value columns gives lo_j = d_4j + 2^8 d_4j+1 and hi_j = d_4j+2 +
+        // 2^8 d_4j+3 (column sums d <= 256 * 255^2, so both are below 2^32), and the value
+        // is sum_j lo_j 2^(32j) + sum_j hi_j 2^(32j+16).  Word j of the second sum is the
+        // funnel shift of hi_j and hi_j-1, so the value is one add-with-carry chain, run
+        // four words per TMEM load; the 8 columns after the value give the nearest quotient.
         if (warp < 4) {
-        uint32_t acc[W + 2];
-        uint64_t carry = 0;
-        uint64_t fsum0 = 0, fsum1 = 0;
+            constexpr int NW = NV / 4;  // value words (W + 1)
+            uint32_t acc[W + 2];
+            uint32_t cy = 0, prev_hi = 0;
+            uint64_t fsum0 = 0, fsum1 = 0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            uint32_t d[16];
-            tc::tmem_ld16(taddr + 16 * q, d);
-            tc::tmem_wait_ld();
+            for (int q2 = 0; q2 < 4; ++q2) {
+                uint32_t d[2][16];
+                tc::tmem_ld16(taddr + 32 * q2, d[0]);
+                tc::tmem_ld16(taddr + 32 * q2 + 16, d[1]);
+                tc::tmem_wait_ld();
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int J = 16 * q + 4 * u;  // first byte column of this 32-bit word
-                // column sums d <= 256 * 255^2: d0 + 2^8 d1 and d2 + 2^8 d3 are below 2^32
-                const uint32_t lo = d[4 * u] + (d[4 * u + 1] << 8), hi = d[4 * u + 2] + (d[4 * u + 3] << 8);
-                const uint64_t s = uint64_t(lo) + (uint64_t(hi) << 16);
-                if (J < NV) {
-                    const uint64_t x = s + carry;
-                    acc[J / 4] = uint32_t(x);
-                    carry = x >> 32;
-                } else if (J == NV) {
-                    fsum0 = s;
-                } else if (J == NV + 4) {
-                    fsum1 = s;
+                for (int h = 0; h < 2; ++h) {
+                    const int j0 = 8 * q2 + 4 * h;  // first word of this load
+                    uint32_t lo[4], hi[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        lo[u] = d[h][4 * u] + (d[h][4 * u + 1] << 8);
+                        hi[u] = d[h][4 * u + 2] + (d[h][4 * u + 3] << 8);
+                    }
+                    if (j0 + 4 <= NW) {
+                        uint32_t b[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            b[u] = __funnelshift_l(u ? hi[u - 1] : prev_hi, hi[u], 16);
+                            acc[j0 + u] = lo[u];
+                        }
+                        add4_carry(acc[j0], acc[j0 + 1], acc[j0 + 2], acc[j0 + 3], b, cy);
+                        prev_hi = hi[3];
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int j = j0 + u;
+                            if (j < NW) {
+                                acc[j] = lo[u];
+                                add1_carry(acc[j], __funnelshift_l(prev_hi, hi[u], 16), cy);
+                                prev_hi = hi[u];
+                            } else if (j == NW) {
+                                fsum0 = uint64_t(lo[u]) + (uint64_t(hi[u]) << 16);
+                            } else if (j == NW + 1) {
+                                fsum1 = uint64_t(lo[u]) + (uint64_t(hi[u]) << 16);
+                            }
+                        }
+                    }
                 }
             }
-        }
-        acc[W + 1] = uint32_t(carry);
-        const uint64_t f1 = fsum1 + (fsum0 >> 32);
-        // nearest integer of sum t_i / p_i: (f1 * 2^32 + low) / 2^64 rounded
-        const uint32_t nearest = uint32_t(f1 >> 32) + (uint32_t(f1) >> 31);
-        const int rr = tid / Gc, cc = tid % Gc;
-        if (rr < R) {
-            const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
-            crt_finish<W, RED>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride, t.ktab);
-        }
+            static_assert(NW + 2 <= 32 && NW == W + 1, "value words and quotient columns fill the 128 TMEM columns");
+            acc[W + 1] = cy + (prev_hi >> 16);
+            const uint64_t f1 = fsum1 + (fsum0 >> 32);
+            // nearest integer of sum t_i / p_i: (f1 * 2^32 + low) / 2^64 rounded
+            const uint32_t nearest = uint32_t(f1 >> 32) + (uint32_t(f1) >> 31);
+            const int rr = tid / Gc, cc = tid % Gc;
+            if (rr < R) {
+                const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
+                // the weights are reduced mod q: the value is below 4P 255 q < 2^32 q
+                crt_finish<W, RED, true>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride,
+                                         t.ktab);
+            }
         }
         tc::fence_before();
         __syncthreads();
