@@ -291,6 +291,7 @@ struct BatchCore {
             d.consts = p->d_consts;
             d.ktab = p->d_ktab;
             d.crt_w = p->d_crt_weights;
+            d.kfrac = p->d_kfrac;
             plans.push_back(std::move(p));
         }
         io_words = io;

@@ -490,6 +490,50 @@ __device__ __forceinline__ void reduce_special(uint32_t (&v)[W + 2], const uint3
 // the one delta selects at run time (kernels whose products may be either).
 enum CrtReduction { kReduceGeneral = 0, kReduceSpecial = 1, kReduceEither = 2 };
 
+// One output coefficient: v[0..W) and zero words up to its stride.
+template <int W>
+__device__ __forceinline__ void store_coef(const uint32_t (&v)[W + 2], uint32_t* dst, int stride) {
+    if ((stride & 3) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+#pragma unroll
+        for (int k = 0; k < W; k += 4)
+            if (k < stride) *reinterpret_cast<uint4*>(dst + k) = make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+        for (int k = W; k < stride; k += 4) *reinterpret_cast<uint4*>(dst + k) = make_uint4(0, 0, 0, 0);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < W; k += 2)
+        if (k < stride) *reinterpret_cast<uint2*>(dst + k) = make_uint2(v[k], v[k + 1]);
+    for (int k = W; k < stride; ++k) dst[k] = 0;
+}
+
+// v in [0, 2q) -> [0, q).  v >= q needs a non-zero word W or W+1, or top four words
+// (W-4 .. W-1, which hold q's top non-zero word) at least q's: a four-word compare
+// decides, and the full subtraction runs only then -- rarely, when the quotient
+// estimate was one low.
+template <int W>
+__device__ __forceinline__ void final_sub_q(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q) {
+    static_assert(W >= 4 && W % 4 == 0, "q words come in fours");
+    uint32_t borrow = 0;
+    asm("sub.cc.u32 %0, %1, %5;\n\t"
+        "subc.cc.u32 %0, %2, %6;\n\t"
+        "subc.cc.u32 %0, %3, %7;\n\t"
+        "subc.cc.u32 %0, %4, %8;\n\t"
+        "subc.u32 %0, 0, 0;"
+        : "+r"(borrow)
+        : "r"(v[W - 4]), "r"(v[W - 3]), "r"(v[W - 2]), "r"(v[W - 1]), "r"(q[W - 4]), "r"(q[W - 3]), "r"(q[W - 2]),
+          "r"(q[W - 1]));
+    if ((v[W] | v[W + 1]) == 0 && borrow != 0) return;
+    uint32_t qq[W + 2], d[W + 2];
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) {
+        qq[k] = k < W ? q[k] : 0u;
+        d[k] = v[k];
+    }
+    const uint32_t borrowed = mp_sub<W + 2>(d, qq);
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) v[k] = borrowed ? v[k] : d[k];
+}
+
 // Final CRT step shared by the SIMT and tensor paths: v += nearest *
 // (-P mod q), reduce mod q, store one coefficient (stride words).  With ktab
 // (rows k = 0 .. 2P of k (-P mod q) mod q, W words each, 16-byte aligned) the
@@ -528,17 +572,7 @@ __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t neares
         else
             reduce_mod_q<W, SMALLQ>(v, s_q, mu_q, sbits);
     }
-    if ((stride & 3) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-#pragma unroll
-        for (int k = 0; k < W; k += 4)
-            if (k < stride) *reinterpret_cast<uint4*>(dst + k) = make_uint4(v[k], v[k + 1], v[k + 2], v[k + 3]);
-        for (int k = W; k < stride; k += 4) *reinterpret_cast<uint4*>(dst + k) = make_uint4(0, 0, 0, 0);
-        return;
-    }
-#pragma unroll
-    for (int k = 0; k < W; k += 2)
-        if (k < stride) *reinterpret_cast<uint2*>(dst + k) = make_uint2(v[k], v[k + 1]);
-    for (int k = W; k < stride; ++k) dst[k] = 0;
+    store_coef<W>(v, dst, stride);
 }
 
 // ---------------------------------------------------------------------------

@@ -151,6 +151,7 @@ struct PlanCore {
     cudaStream_t stream = nullptr;
     // tensor path constants
     uint8_t* d_crt_weights = nullptr;
+    uint64_t* d_kfrac = nullptr;   // [2P+1] floor(2^64 (k (-P_total mod q) mod q) / q)
     uint32_t* d_err = nullptr;     // set by a kernel whose bounded wait ran out
     uint32_t tensor_k_crt = 0;
 

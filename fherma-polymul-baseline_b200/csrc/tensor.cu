@@ -46,7 +46,7 @@ std::vector<uint8_t> conversion_image(const std::vector<uint32_t>& primes) {
 
 void tensor_init(PlanCore& s) {
     if (uint32_t(s.P) * 4 > uint32_t(tc::kCrtK)) throw Failure(PM_ERR_UNSUPPORTED, "prime basis too large for the CRT tile");
-    if (4 * s.W + 4 + 8 > uint32_t(tc::kCrtN)) throw Failure(PM_ERR_UNSUPPORTED, "q too wide for the CRT tile");
+    if (4 * s.W + 16 > uint32_t(tc::kCrtN)) throw Failure(PM_ERR_UNSUPPORTED, "q too wide for the CRT tile");
     if (s.stride % 4) throw Failure(PM_ERR_UNSUPPORTED, "tensor path needs an even coef_limbs (16-byte coefficient rows)");
     DeviceBasis& B = *s.basis;
     {
@@ -60,10 +60,11 @@ void tensor_init(PlanCore& s) {
         }
     }
     // CRT weights: [2 K-atoms][128 rows][128 B].  Row (i, a) holds the bytes of
-    // ((P/p_i) mod q) 2^(8a) mod q: digit byte a of t_i times it sums, over a, to
-    // t_i (P/p_i) mod q, and the whole contraction stays below 4P 255 q < 2^16 q,
-    // so the CRT's final reduction removes a one-word quotient.
-    const uint32_t NV = 4 * s.W + 4;
+    // w_ia = ((P/p_i) mod q) 2^(8a) mod q: digit byte a of t_i times it sums, over a, to
+    // t_i (P/p_i) mod q, and the contraction V = sum byte_a(t_i) w_ia stays below 4P 255 q.
+    // Columns: 4W value bytes, then 8 bytes of floor(2^64 / p_i) 2^(8a) (the nearest
+    // quotient k of sum t_i / p_i), then 8 bytes of floor(2^64 w_ia / q) (V / q to 2^-40).
+    const uint32_t NV = 4 * s.W;
     Words total{1};
     for (unsigned i = 0; i < s.P; ++i) total = multiply_small(total, B.primes[i]);
     std::vector<uint8_t> img(32768, 0);
@@ -73,23 +74,43 @@ void tensor_init(PlanCore& s) {
         const Words mq = mod(m, s.q);
         const uint64_t recip = uint64_t(((unsigned __int128)1 << 64) / B.primes[i]);
         for (int a = 0; a < 4; ++a) {
-            const Words shifted = mod(shift_left(mq, 8 * a), s.q);
+            const Words w = mod(shift_left(mq, 8 * a), s.q);
+            Words f;
+            divmod(shift_left(w, 64), s.q, &f, nullptr);
+            const Words f64 = padded(f, 2);
             const unsigned __int128 rs = (unsigned __int128)recip << (8 * a);
             const uint32_t k = 4 * i + a, ka = k >> 7, kk = k & 127;
             for (uint32_t J = 0; J < NV; ++J) {
-                const uint32_t word = J / 4 < shifted.size() ? shifted[J / 4] : 0;
+                const uint32_t word = J / 4 < w.size() ? w[J / 4] : 0;
                 img[ka * 16384 + tc::sw128_offset(J, kk)] = uint8_t(word >> (8 * (J % 4)));
             }
-            for (uint32_t J = 0; J < 8; ++J) img[ka * 16384 + tc::sw128_offset(NV + J, kk)] = uint8_t(rs >> (8 * J));
+            for (uint32_t J = 0; J < 8; ++J) {
+                img[ka * 16384 + tc::sw128_offset(NV + J, kk)] = uint8_t(rs >> (8 * J));
+                img[ka * 16384 + tc::sw128_offset(NV + 8 + J, kk)] = uint8_t(f64[J / 4] >> (8 * (J % 4)));
+            }
         }
     }
     cuda_check(cudaMalloc(&s.d_crt_weights, img.size()), "allocate CRT weights");
     cuda_check(cudaMemcpy(s.d_crt_weights, img.data(), img.size(), cudaMemcpyHostToDevice), "upload CRT weights");
+    // floor(2^64 (row k of the k table) / q), which joins the estimate of V / q
+    const Words pmod = mod(total, s.q);
+    const Words pneg = compare(pmod, Words{}) == 0 ? Words{} : subtract(s.q, pmod);
+    std::vector<uint64_t> kfrac(2 * size_t(s.P) + 1, 0);
+    for (unsigned k = 1; k <= 2 * s.P; ++k) {
+        Words f;
+        divmod(shift_left(mod(multiply_small(pneg, k), s.q), 64), s.q, &f, nullptr);
+        const Words f64 = padded(f, 2);
+        kfrac[k] = uint64_t(f64[0]) | (uint64_t(f64[1]) << 32);
+    }
+    cuda_check(cudaMalloc(&s.d_kfrac, kfrac.size() * 8), "allocate CRT fractions");
+    cuda_check(cudaMemcpy(s.d_kfrac, kfrac.data(), kfrac.size() * 8, cudaMemcpyHostToDevice), "upload CRT fractions");
 }
 
 void tensor_release(PlanCore& s) {
     cudaFree(s.d_crt_weights);
     s.d_crt_weights = nullptr;
+    cudaFree(s.d_kfrac);
+    s.d_kfrac = nullptr;
 }
 
 namespace {
@@ -215,8 +236,8 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     int ctas = s.sms * s.tune.crt_ctas_per_sm;
     if (ctas > items) ctas = items;
     const size_t smem = k3t_smem_bytes<LOGR>();
-    // one plan, one q: the reduction is chosen here rather than per coefficient
-    auto kernel = s.delta ? k3t_crt<LOGR, W, PlanCrtWork, kReduceSpecial> : k3t_crt<LOGR, W, PlanCrtWork, kReduceGeneral>;
+    // the reduction mod q is a table row: the same kernel for a special-form q
+    auto kernel = k3t_crt<LOGR, W, PlanCrtWork>;
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K3T shared memory");
     PlanCrtWork w;
@@ -231,6 +252,7 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     w.consts = s.d_consts;
     w.ktab = s.d_ktab;
     w.crt_w = s.d_crt_weights;
+    w.kfrac = s.d_kfrac;
     w.mu_q = s.mu_q;
     w.sbits = int(s.qbits);
     w.delta = s.delta;

@@ -61,6 +61,7 @@ struct CrtTarget {
     const uint32_t* consts;  // q[W], (-P mod q)[W]
     const uint32_t* ktab;    // [2P+1][W] k (-P mod q) mod q
     const uint8_t* crt_w;    // [2][128][128] pre-swizzled CRT weights
+    const uint64_t* kfrac;   // [2P+1] floor(2^64 (row k of ktab) / q)
     uint64_t mu_q;
     int sbits, n, logC, P, stride, use_tma;
     uint32_t delta;          // special-form q = 2^sbits - delta, or 0
@@ -77,6 +78,7 @@ struct BatchProduct {
     const uint32_t* consts;
     const uint32_t* ktab;
     const uint8_t* crt_w;
+    const uint64_t* kfrac;
 };
 
 struct PlanConvWork {
@@ -144,6 +146,7 @@ struct PlanCrtWork {
     const uint32_t* consts;
     const uint32_t* ktab;
     const uint8_t* crt_w;
+    const uint64_t* kfrac;
     uint64_t mu_q;
     int sbits, n, logC, P, stride, count, use_tma;
     uint32_t delta;
@@ -152,7 +155,7 @@ struct PlanCrtWork {
     __device__ int2 item(int k) const { return make_int2(k >> lg(), k & ((1 << lg()) - 1)); }
     __device__ CrtTarget target(int z) const {
         return CrtTarget{&map_res, z, work + z * ws_bstride, out + z * io_bstride, scale, consts, ktab, crt_w,
-                         mu_q, sbits, n, logC, P, stride, use_tma, delta};
+                         kfrac, mu_q, sbits, n, logC, P, stride, use_tma, delta};
     }
 };
 
@@ -171,7 +174,7 @@ struct TableCrtWork {
     __device__ CrtTarget target(int z) const {
         const BatchProduct& d = prod[z];
         return CrtTarget{maps + 3 * z + 2, 0, work + d.ws_off, out + d.io_off, d.scale, d.consts, d.ktab, d.crt_w,
-                         d.mu_q, d.sbits, d.n, d.logC, d.P, d.stride, 1, d.delta};
+                         d.kfrac, d.mu_q, d.sbits, d.n, d.logC, d.P, d.stride, 1, d.delta};
     }
 };
 
@@ -445,12 +448,13 @@ __device__ __forceinline__ void add1_carry(uint32_t& a, uint32_t b, uint32_t& cy
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB,
 // residue box 64*R*8 words, inverse column twiddles 64*(R-1) uint2.
 // ---------------------------------------------------------------------------
-template <int LOGR, int W, class Work, int RED = kReduceEither>
+template <int LOGR, int W, class Work>
 __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs,
                                                const uint2* __restrict__ tw_inv, uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
     constexpr int RT = R > 1 ? R - 1 : 1;
-    constexpr int NV = 4 * W + 4;  // value byte columns
+    constexpr int NV = 4 * W;  // value byte columns, then 8 + 8 quotient-estimate columns
+    static_assert(NV + 16 <= tc::kCrtN, "value and estimate columns fill at most the 128 TMEM columns");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = sbase;                                        // [2][128][128 B]
@@ -459,9 +463,10 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
     uint2* sTw = reinterpret_cast<uint2*>(sR + tc::kMaxPrimes * R * 8);  // [P][R-1]
     __shared__ uint64_t tma_bar, mma_bar;
     __shared__ uint32_t tmem_base;
-    __shared__ uint32_t s_q[2 * W];
+    __shared__ __align__(16) uint32_t s_q[2 * W];
     __shared__ uint32_t s_p[tc::kMaxPrimes];                // the product's primes
     __shared__ uint2 s_sc[2 * tc::kMaxPrimes];              // its CRT scales s_i, then s_i psi_i^-brev(1)
+    __shared__ uint64_t s_kf[2 * tc::kMaxPrimes + 1];       // floor(2^64 (row k of its k table) / q)
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int total = w.total();
@@ -505,6 +510,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             const uint4* src = reinterpret_cast<const uint4*>(t.crt_w);
             for (int q = tid; q < 2048; q += tc::kCrtThreads) reinterpret_cast<uint4*>(sB)[q] = __ldg(src + q);
             for (int q = tid; q < 2 * W; q += tc::kCrtThreads) s_q[q] = t.consts[q];
+            for (int q = tid; q <= 2 * t.P; q += tc::kCrtThreads) s_kf[q] = __ldg(t.kfrac + q);
             for (int q = tid; q < t.P; q += tc::kCrtThreads) {
                 s_p[q] = __ldg(&pcs[q].p);
                 s_sc[q] = __ldg(t.scale + q);
@@ -596,68 +602,86 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         mma_phase ^= 1;
         tc::fence_after();
         // --- the CRT value of row m = tid (warps 0-3, the TMEM lane owners) ---
-        // Word j of the value columns gives lo_j = d_4j + 2^8 d_4j+1 and hi_j = d_4j+2 +
-        // 2^8 d_4j+3 (column sums d <= 256 * 255^2, so both are below 2^32), and the value
-        // is sum_j lo_j 2^(32j) + sum_j hi_j 2^(32j+16).  Word j of the second sum is the
-        // funnel shift of hi_j and hi_j-1, so the value is one add-with-carry chain, run
-        // four words per TMEM load; the 8 columns after the value give the nearest quotient.
         if (warp < 4) {
-            constexpr int NW = NV / 4;  // value words (W + 1)
+            // The 16 estimate columns first.  Columns NV..NV+7 give sum t_i floor(2^64/p_i),
+            // whose nearest integer over 2^64 is the CRT's k; columns NV+8..NV+15 give
+            // sum byte_a(t_i) floor(2^64 w_ia / q), 2^64 V/q less under 2^-40 of a unit.
+            // With G_k = floor(2^64 (row k) / q) added, the integer part Q is the quotient
+            // of V + row k by q, or one less: V + row k - Q q lies in [0, 2q).
+            uint32_t e[16];
+            tc::tmem_ld16(taddr + NV, e);
+            tc::tmem_wait_ld();
+            uint64_t fs[4];  // four-column sums, below 2^48
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                fs[u] = uint64_t(e[4 * u] + (e[4 * u + 1] << 8)) + (uint64_t(e[4 * u + 2] + (e[4 * u + 3] << 8)) << 16);
+            const uint64_t fk = fs[1] + (fs[0] >> 32);
+            const uint32_t k = min(uint32_t(fk >> 32) + (uint32_t(fk) >> 31), uint32_t(2 * t.P));
+            const uint64_t gk = s_kf[k];
+            const uint64_t low = (fs[2] & 0xffffffffull) + (gk & 0xffffffffull);
+            const uint32_t Q = uint32_t((fs[3] + (fs[2] >> 32) + (gk >> 32) + (low >> 32)) >> 32);
+            const uint4* krow = reinterpret_cast<const uint4*>(t.ktab + size_t(k) * W);
+            // Word j of the value columns gives lo_j = d_4j + 2^8 d_4j+1 and hi_j = d_4j+2 +
+            // 2^8 d_4j+3 (column sums d <= 256 * 255^2, so both are below 2^32), and V is
+            // sum_j lo_j 2^(32j) + sum_j hi_j 2^(32j+16).  Word j of the second sum is the
+            // funnel shift of hi_j and hi_j-1, so V is one add-with-carry chain, run four
+            // words per TMEM load.
             uint32_t acc[W + 2];
             uint32_t cy = 0, prev_hi = 0;
-            uint64_t fsum0 = 0, fsum1 = 0;
 #pragma unroll
-            for (int q2 = 0; q2 < 4; ++q2) {
+            for (int q2 = 0; q2 < (NV + 31) / 32; ++q2) {
                 uint32_t d[2][16];
                 tc::tmem_ld16(taddr + 32 * q2, d[0]);
-                tc::tmem_ld16(taddr + 32 * q2 + 16, d[1]);
+                if (32 * q2 + 16 < NV) tc::tmem_ld16(taddr + 32 * q2 + 16, d[1]);
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int j0 = 8 * q2 + 4 * h;  // first word of this load
-                    uint32_t lo[4], hi[4];
+                    if (j0 >= W) break;
+                    uint32_t b[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        lo[u] = d[h][4 * u] + (d[h][4 * u + 1] << 8);
-                        hi[u] = d[h][4 * u + 2] + (d[h][4 * u + 3] << 8);
+                        const uint32_t lo = d[h][4 * u] + (d[h][4 * u + 1] << 8);
+                        const uint32_t hi = d[h][4 * u + 2] + (d[h][4 * u + 3] << 8);
+                        b[u] = __funnelshift_l(prev_hi, hi, 16);
+                        acc[j0 + u] = lo;
+                        prev_hi = hi;
                     }
-                    if (j0 + 4 <= NW) {
-                        uint32_t b[4];
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            b[u] = __funnelshift_l(u ? hi[u - 1] : prev_hi, hi[u], 16);
-                            acc[j0 + u] = lo[u];
-                        }
-                        add4_carry(acc[j0], acc[j0 + 1], acc[j0 + 2], acc[j0 + 3], b, cy);
-                        prev_hi = hi[3];
-                    } else {
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int j = j0 + u;
-                            if (j < NW) {
-                                acc[j] = lo[u];
-                                add1_carry(acc[j], __funnelshift_l(prev_hi, hi[u], 16), cy);
-                                prev_hi = hi[u];
-                            } else if (j == NW) {
-                                fsum0 = uint64_t(lo[u]) + (uint64_t(hi[u]) << 16);
-                            } else if (j == NW + 1) {
-                                fsum1 = uint64_t(lo[u]) + (uint64_t(hi[u]) << 16);
-                            }
-                        }
-                    }
+                    add4_carry(acc[j0], acc[j0 + 1], acc[j0 + 2], acc[j0 + 3], b, cy);
                 }
             }
-            static_assert(NW + 2 <= 32 && NW == W + 1, "value words and quotient columns fill the 128 TMEM columns");
-            acc[W + 1] = cy + (prev_hi >> 16);
-            const uint64_t f1 = fsum1 + (fsum0 >> 32);
-            // nearest integer of sum t_i / p_i: (f1 * 2^32 + low) / 2^64 rounded
-            const uint32_t nearest = uint32_t(f1 >> 32) + (uint32_t(f1) >> 31);
+            acc[W] = cy + (prev_hi >> 16);
+            acc[W + 1] = 0;
+            uint32_t row[W + 2];
+#pragma unroll
+            for (int u = 0; u < W / 4; ++u) {
+                const uint4 x = __ldg(krow + u);
+                row[4 * u] = x.x;
+                row[4 * u + 1] = x.y;
+                row[4 * u + 2] = x.z;
+                row[4 * u + 3] = x.w;
+            }
+            row[W] = row[W + 1] = 0;
+            mp_add<W + 2>(acc, row);
+            // minus Q q: one W-word multiply-accumulate (Q < 2^16)
+            uint32_t qw[W];
+#pragma unroll
+            for (int u = 0; u < W / 4; ++u) {
+                const uint4 x = reinterpret_cast<const uint4*>(s_q)[u];
+                qw[4 * u] = x.x;
+                qw[4 * u + 1] = x.y;
+                qw[4 * u + 2] = x.z;
+                qw[4 * u + 3] = x.w;
+            }
+#pragma unroll
+            for (int u = 0; u < W + 2; ++u) row[u] = 0;
+            crt_mac<W>(row, Q, qw);
+            mp_sub<W + 2>(acc, row);
+            final_sub_q<W>(acc, s_q);
             const int rr = tid / Gc, cc = tid % Gc;
             if (rr < R) {
                 const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
-                // the weights are reduced mod q: the value is below 4P 255 q < 2^32 q
-                crt_finish<W, RED, true>(acc, nearest, s_q, t.mu_q, t.sbits, t.delta, t.out + J * t.stride, t.stride,
-                                         t.ktab);
+                store_coef<W>(acc, t.out + J * t.stride, t.stride);
             }
         }
         tc::fence_before();
