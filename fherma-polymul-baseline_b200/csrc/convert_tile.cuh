@@ -40,16 +40,20 @@ struct TileItem {
     int z, poly, cg;
 };
 
-// `count` products of one plan: items (z, poly, cg) numbered product-major.
+// `count` products of one plan: items (z, poly, cg) numbered product-major; with
+// poly_only = 0 or 1, the items of that polynomial alone (its conversion can start
+// while the other polynomial is still arriving).
 struct PlanTileWork {
     CUtensorMap map_a, map_b;
     uint32_t* work;
     size_t ws_bstride;
     int n, logC, P, count;
+    int poly_only;  // -1: both polynomials
     __device__ int lg() const { return logC - min(logC, 3); }  // column groups per row = 2^lg
-    __device__ int total() const { return count << (lg() + 1); }
+    __device__ int total() const { return count << (lg() + (poly_only < 0 ? 1 : 0)); }
     __device__ TileItem item(int k) const {
         const int g = lg();
+        if (poly_only >= 0) return TileItem{k >> g, poly_only, k & ((1 << g) - 1)};
         return TileItem{k >> (g + 1), (k >> g) & 1, k & ((1 << g) - 1)};
     }
     __device__ ConvTarget target(int z, int poly) const {

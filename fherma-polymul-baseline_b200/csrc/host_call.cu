@@ -12,7 +12,9 @@
 //     overlap (the reference gets the same overlap from its copy pool and
 //     4-chunk input pipeline, host_copy_pool.h, input_pipeline.h:12-54,
 //     rns/solve.cu:731-761);
-//   - the kernels follow on the same stream; the product comes back in
+//   - a's conversion starts on a side stream as soon as a's copies are queued,
+//     so it runs while b is still on the link; b's conversion, the row and the
+//     CRT kernels follow on the plan's stream; the product comes back in
 //     pieces, each with an event, and the pool copies piece k out as soon as
 //     its event fires, while later pieces are still on the link;
 //   - the call is split (begin / end) so that a caller can do its own work --
@@ -314,6 +316,12 @@ void piece(size_t bytes, int pieces, int k, size_t* off, size_t* len) {
 
 HostCall::~HostCall() {
     if (stream) cudaStreamSynchronize(stream);
+    if (side) {
+        cudaStreamSynchronize(side);
+        cudaStreamDestroy(side);
+    }
+    if (a_in) cudaEventDestroy(a_in);
+    if (a_converted) cudaEventDestroy(a_converted);
     for (auto& e : out_ready)
         if (e) cudaEventDestroy(e);
     cudaFree(d_io);
@@ -331,6 +339,9 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
         cuda_check(cudaMallocHost(&h.h_stage, 3 * s.io_bytes + 64), "allocate pinned staging");
         h.out_ready.assign(kOutPieces, nullptr);
         for (auto& e : h.out_ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "output events");
+        cuda_check(cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking), "conversion stream");
+        cuda_check(cudaEventCreateWithFlags(&h.a_in, cudaEventDisableTiming), "input event");
+        cuda_check(cudaEventCreateWithFlags(&h.a_converted, cudaEventDisableTiming), "conversion event");
     }
     if (!h.pool) h.pool = std::make_unique<CopyPool>(pool_threads());
     const size_t io = s.io_bytes;
@@ -338,10 +349,24 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
     uint8_t* stage = static_cast<uint8_t*>(h.h_stage);
     const uint8_t* src[2] = {reinterpret_cast<const uint8_t*>(a), reinterpret_cast<const uint8_t*>(b)};
     const bool pinned[2] = {is_pinned(a), is_pinned(b)};
+    // Where the plan converts one polynomial at a time, a's conversion runs on the side
+    // stream as soon as a's copies are queued, while b is still on the link.
+    const bool split = conversion_splits(s);
+    uint32_t* work = s.d_work;
+    bool a_aside = false;
+    auto convert_a_aside = [&]() {
+        cuda_check(cudaEventRecord(h.a_in, h.stream), "input event");
+        cuda_check(cudaStreamWaitEvent(h.side, h.a_in, 0), "conversion stream wait");
+        launch_tensor_convert_poly(s, reinterpret_cast<const uint32_t*>(dev), 0, work, h.side);
+        cuda_check(cudaEventRecord(h.a_converted, h.side), "conversion event");
+        a_aside = true;
+    };
     // pinned inputs go straight to the link in one copy each
     for (int poly = 0; poly < 2; ++poly)
-        if (pinned[poly])
+        if (pinned[poly]) {
             cuda_check(cudaMemcpyAsync(dev + poly * io, src[poly], io, cudaMemcpyHostToDevice, h.stream), "copy in");
+            if (split && poly == 0) convert_a_aside();
+        }
     // pageable inputs: the pool's threads stage the units (in index order, as they take
     // them) while this thread queues each copy group as soon as its units are staged -- one
     // thread talks to the runtime, so the copies enter the stream without contending
@@ -369,6 +394,8 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
                 cuda_check(cudaMemcpyAsync(dst, stage + g.poly[grp] * io + off, g.len[grp], cudaMemcpyHostToDevice,
                                            h.stream),
                            "copy in");
+                if (split && !a_aside && g.poly[grp] == 0 && (grp + 1 == g.count || g.poly[grp + 1] != 0))
+                    convert_a_aside();
             }
         } catch (...) {
             try {
@@ -379,8 +406,14 @@ void multiply_host_begin(PlanCore& s, const uint64_t* a, const uint64_t* b, uint
         }
         h.pool->finish();
     }
-    launch_product(s, reinterpret_cast<const uint64_t*>(dev), reinterpret_cast<const uint64_t*>(dev + io),
-                   reinterpret_cast<uint64_t*>(dev + 2 * io), nullptr, h.stream);
+    if (a_aside) {
+        launch_tensor_convert_poly(s, reinterpret_cast<const uint32_t*>(dev + io), 1, work, h.stream);
+        cuda_check(cudaStreamWaitEvent(h.stream, h.a_converted, 0), "conversion wait");
+        launch_tensor_after_conversion(s, reinterpret_cast<uint32_t*>(dev + 2 * io), work, 1, h.stream);
+    } else {
+        launch_product(s, reinterpret_cast<const uint64_t*>(dev), reinterpret_cast<const uint64_t*>(dev + io),
+                       reinterpret_cast<uint64_t*>(dev + 2 * io), nullptr, h.stream);
+    }
     // a pinned output takes the product directly; otherwise it lands in the staging
     h.direct_out = direct_out && is_pinned(direct_out) ? reinterpret_cast<uint8_t*>(direct_out) : nullptr;
     uint8_t* land = h.direct_out ? h.direct_out : stage + 2 * io;

@@ -72,6 +72,8 @@ struct PipelineSlot {
 class CopyPool;
 struct HostCall {
     cudaStream_t stream = nullptr;  // the plan's stream
+    cudaStream_t side = nullptr;    // converts a while b is on the link
+    cudaEvent_t a_in = nullptr, a_converted = nullptr;
     void* d_io = nullptr;           // a, b, c on the device
     void* h_stage = nullptr;        // pinned a, b, c and the error word
     std::vector<cudaEvent_t> out_ready;
@@ -224,6 +226,11 @@ void tensor_release(PlanCore& s);
 void quartic_init(PlanCore& s);
 void launch_quartic(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
                     uint32_t count, cudaStream_t st);
+// The single-product host call's split: conversion of one polynomial (K1W plans only:
+// conversion_splits), then the row and CRT kernels once both are converted.
+bool conversion_splits(const PlanCore& s);
+void launch_tensor_convert_poly(const PlanCore& s, const uint32_t* x, int poly, uint32_t* work, cudaStream_t st);
+void launch_tensor_after_conversion(const PlanCore& s, uint32_t* c, uint32_t* work, uint32_t count, cudaStream_t st);
 void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
                    uint32_t count, cudaStream_t st);
 

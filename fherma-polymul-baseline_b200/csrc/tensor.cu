@@ -190,9 +190,9 @@ void launch_k1t(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
 // the whole basis per tile: two CTAs per SM, contiguous runs of items
 template <int LOGR>
 void launch_k1w(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* work, uint32_t count,
-                cudaStream_t st) {
+                cudaStream_t st, int poly_only = -1) {
     const int C = 1 << s.logC, Gc = C < 8 ? C : 8;
-    const int items = int(count) * 2 * (C / Gc);
+    const int items = int(count) * (poly_only < 0 ? 2 : 1) * (C / Gc);
     int ctas = s.sms * 2;
     if (ctas > items) ctas = items;
     const size_t smem = k1w_smem_bytes();
@@ -200,8 +200,9 @@ void launch_k1w(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
                                     int(smem)),
                "K1W shared memory");
     PlanTileWork w;
-    w.map_a = coefficient_map(s, a, count);
-    w.map_b = coefficient_map(s, b, count);
+    w.poly_only = poly_only;
+    w.map_a = coefficient_map(s, poly_only == 1 ? b : a, count);
+    w.map_b = poly_only == 0 ? w.map_a : coefficient_map(s, b, count);
     w.work = work;
     w.ws_bstride = s.workspace_bytes / 4;
     w.n = int(s.n);
@@ -339,6 +340,46 @@ void launch_quartic(const PlanCore& s, const uint32_t* a, const uint32_t* b, uin
     }
     cuda_check(cudaGetLastError(), "launch quartic product kernels");
     count_launches(3);
+}
+
+bool conversion_splits(const PlanCore& s) {
+    return (s.flags & PM_CONVERT_TENSOR) && !s.quartic && !s.wide && s.tune.conv_whole_basis;
+}
+
+void launch_tensor_convert_poly(const PlanCore& s, const uint32_t* x, int poly, uint32_t* work, cudaStream_t st) {
+    if (!conversion_splits(s)) throw Failure(PM_ERR_INVALID, "this plan converts both polynomials in one launch");
+    ProfileScope prof("k1t_convert_cols", st);
+    const uint32_t* a = poly == 0 ? x : nullptr;
+    const uint32_t* b = poly == 1 ? x : nullptr;
+    switch (s.logR) {
+        case 0: launch_k1w<0>(s, a, b, work, 1, st, poly); break;
+        case 1: launch_k1w<1>(s, a, b, work, 1, st, poly); break;
+        case 2: launch_k1w<2>(s, a, b, work, 1, st, poly); break;
+        case 3: launch_k1w<3>(s, a, b, work, 1, st, poly); break;
+        default: launch_k1w<4>(s, a, b, work, 1, st, poly); break;
+    }
+    cuda_check(cudaGetLastError(), "launch conversion");
+    count_launches(1);
+}
+
+void launch_tensor_after_conversion(const PlanCore& s, uint32_t* c, uint32_t* work, uint32_t count,
+                                    cudaStream_t st) {
+    {
+        ProfileScope prof("k2_rows", st);
+        launch_rows(s, work, count, st);
+    }
+    {
+        ProfileScope prof("k3t_cols_crt", st);
+        switch (s.logR) {
+            case 0: launch_k3t_w<0>(s, work, c, count, st); break;
+            case 1: launch_k3t_w<1>(s, work, c, count, st); break;
+            case 2: launch_k3t_w<2>(s, work, c, count, st); break;
+            case 3: launch_k3t_w<3>(s, work, c, count, st); break;
+            default: launch_k3t_w<4>(s, work, c, count, st); break;
+        }
+    }
+    cuda_check(cudaGetLastError(), "launch tensor product kernels");
+    count_launches(2);
 }
 
 void launch_tensor(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* work,
