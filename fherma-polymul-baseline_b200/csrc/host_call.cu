@@ -90,16 +90,18 @@ bool is_pinned(const void* p) {
 }  // namespace
 
 // How long an idle copy thread spins before it sleeps: PM_HOST_SPIN_US (microseconds,
-// read once), 2000 by default.  A caller that leaves longer gaps between products (a
-// harness reading its next case from disk) finds the threads asleep and waits for them
-// to wake; a longer spin trades host CPU time for that latency.
+// read once), 20000 by default.  A caller that leaves longer gaps between products finds
+// the threads asleep and waits for them to wake: a harness that writes one case's 3.7 MB
+// result and reads the next case's 7.3 MB between calls spends a few milliseconds there,
+// and with a 2 ms spin its calls took 15 us longer at N = 32768.  The spin costs the
+// pool's threads that long of CPU time after each call; 0 makes them sleep at once.
 static long spin_us() {
     static const long us = [] {
         const char* e = std::getenv("PM_HOST_SPIN_US");
-        if (!e || !*e) return 2000L;
+        if (!e || !*e) return 20000L;
         char* end = nullptr;
         const long v = std::strtol(e, &end, 10);
-        return (end && *end == 0 && v >= 0 && v <= 10000000L) ? v : 2000L;
+        return (end && *end == 0 && v >= 0 && v <= 10000000L) ? v : 20000L;
     }();
     return us;
 }
