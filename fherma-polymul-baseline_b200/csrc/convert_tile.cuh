@@ -71,7 +71,9 @@ struct ByteFix {
 constexpr int kTW = 136;  // transpose row stride (words): 4 primes of a warp's pairs 8 banks apart
 constexpr size_t k1w_smem_bytes() { return 1024 + 32768 + 32768 + size_t(tc::kMaxPrimes) * kTW * 4; }
 
-template <int LOGR, class Work>
+// LOGC > 0: every item's rows hold 2^LOGC values (a plan's launch at a common ring size),
+// so row strides and plane offsets are constants; 0: read from the item.
+template <int LOGR, class Work, int LOGC = 0>
 __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_constant__ Work w,
                                                                     const PrimeConst* __restrict__ pcs,
                                                                     const uint8_t* __restrict__ conv_w,
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
         auto issue = [&](int k, int buf) {
             const TileItem it = w.item(k);
             const ConvTarget t = w.target(it.z, it.poly);
-            const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+            const int C = 1 << (LOGC ? LOGC : t.logC), Gc = C < 8 ? C : 8;
             tc::mbar_expect_tx(&tma_full[buf], 128u * uint32_t(Gc) * uint32_t(R));
             tc::tma_load_4d(sA + buf * 16384, t.map, 0, it.cg * Gc, 0, t.mz, &tma_full[buf]);
         };
@@ -202,7 +204,9 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
         for (int k = begin; k < end; ++k) {
             const TileItem it = w.item(k);
             const ConvTarget t = w.target(it.z, it.poly);
-            const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+            const int logC = LOGC ? LOGC : t.logC;
+            const int C = 1 << logC, Gc = C < 8 ? C : 8;
+            const size_t n = LOGC ? size_t(1) << (LOGR + LOGC) : size_t(t.n);
             ok = tc::mbar_wait(&mma_full, ph_mma) && ok;
             ph_mma ^= 1u;
             tc::fence_after();
@@ -252,8 +256,8 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
                     for (int r = 0; r < R; ++r)
                         if (!(r & h)) ct_bfly(v[r], v[r + h], stw[i][(1 << s) + (r >> (LOGR - s)) - 1], p, two_p);
                 }
-                uint32_t* dst = t.res + (size_t(it.poly) * P + i) * t.n + size_t(it.cg) * Gc + c;
-                const size_t rowstride = size_t(1) << t.logC;
+                uint32_t* dst = t.res + (size_t(it.poly) * P + i) * n + size_t(it.cg) * Gc + c;
+                const size_t rowstride = size_t(1) << logC;
 #pragma unroll
                 for (int r = 0; r < R; ++r, dst += rowstride) *dst = v[r];
             }

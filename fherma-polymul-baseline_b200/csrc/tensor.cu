@@ -196,8 +196,12 @@ void launch_k1w(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
     int ctas = s.sms * 2;
     if (ctas > items) ctas = items;
     const size_t smem = k1w_smem_bytes();
-    cuda_check(cudaFuncSetAttribute(k1w_convert<LOGR, PlanTileWork>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(smem)),
+    // rows of 1024, 2048 or 4096 values (n = 16384 .. 65536): a kernel with that row length built in
+    auto kernel = k1w_convert<LOGR, PlanTileWork>;
+    if (LOGR == 4 && s.logC == 10) kernel = k1w_convert<LOGR, PlanTileWork, 10>;
+    if (LOGR == 4 && s.logC == 11) kernel = k1w_convert<LOGR, PlanTileWork, 11>;
+    if (LOGR == 4 && s.logC == 12) kernel = k1w_convert<LOGR, PlanTileWork, 12>;
+    cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K1W shared memory");
     PlanTileWork w;
     w.poly_only = poly_only;
@@ -217,8 +221,7 @@ void launch_k1w(const PlanCore& s, const uint32_t* a, const uint32_t* b, uint32_
             fix.shift[t] = s.quartic->fix_shift[t];
         }
     }
-    k1w_convert<LOGR, PlanTileWork><<<ctas, tc::kWideThreads, smem, st>>>(w, s.plane_pc(), s.conv_weights(),
-                                                                        s.plane_fwd(), s.d_err, fix);
+    kernel<<<ctas, tc::kWideThreads, smem, st>>>(w, s.plane_pc(), s.conv_weights(), s.plane_fwd(), s.d_err, fix);
 }
 
 template <int LOGR>
