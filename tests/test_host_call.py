@@ -60,3 +60,35 @@ def test_protocol_errors(cuda):
             p.multiply_host_begin(a, b)
         assert e.value.status == polymul.PM_ERR_BUSY
         assert (p.multiply_host_end() == oracle.rns_multiply(a, b, q)).all()
+
+
+def test_pageable_a_with_pinned_b(cuda):
+    """b goes to the link first (pinned, one copy) and a is staged after it: a's
+    conversion on the side stream then waits behind both copies."""
+    torch = cuda
+    n = 32768
+    rng = np.random.default_rng(613)
+    q = random_q(rng, 868)
+    a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
+    want = oracle.rns_multiply(a, b, q)
+    pb = torch.from_numpy(b.view(np.int64)).pin_memory()
+    with polymul.Plan(n, q, coef_limbs=14) as p:
+        for _ in range(2):
+            c = np.zeros_like(a)
+            p.multiply_host_ptr(a.ctypes.data, pb.data_ptr(), c.ctypes.data)
+            assert (c == want).all()
+
+
+@pytest.mark.parametrize("kind", ["k1t", "simt"])
+def test_host_call_without_the_conversion_split(cuda, kind):
+    """Plans whose conversion takes both polynomials in one launch (the per-group
+    tensor conversion K1T, the plain method) run the call unsplit."""
+    n = 4096
+    rng = np.random.default_rng(614)
+    q = random_q(rng, 868)
+    with polymul.Plan(n, q, coef_limbs=14, tensor=(kind == "k1t")) as p:
+        if kind == "k1t":
+            p.set_tuning(conv_whole_basis=0)
+        for _ in range(2):
+            a, b = uniform_below(rng, q, n, 14), uniform_below(rng, q, n, 14)
+            assert (p.multiply_host(a, b) == oracle.rns_multiply(a, b, q)).all()
