@@ -314,9 +314,10 @@ struct BatchCore {
                                  CU_TENSOR_MAP_SWIZZLE_128B);
             maps[3 * z + 1] = encode(CU_TENSOR_MAP_DATA_TYPE_UINT8, d_b + io_off[z], cdims, cstr, cbox,
                                      CU_TENSOR_MAP_SWIZZLE_128B);
-            const cuuint64_t rdims[4] = {C, p.P, R, 1};  // box lands as [row][prime][column]
+            // box lands as [row][64 primes][column]: a constant row stride (primes past P read as zero)
+            const cuuint64_t rdims[4] = {C, p.P, R, 1};
             const cuuint64_t rstr[3] = {C * R * 4, C * 4, p.workspace_bytes};
-            const cuuint32_t rbox[4] = {Gc, p.P, cuuint32_t(R), 1};
+            const cuuint32_t rbox[4] = {Gc, cuuint32_t(tc::kMaxPrimes), cuuint32_t(R), 1};
             maps[3 * z + 2] = encode(CU_TENSOR_MAP_DATA_TYPE_UINT32, d_work + ws_off[z], rdims, rstr, rbox,
                                      CU_TENSOR_MAP_SWIZZLE_NONE);
         }

@@ -151,11 +151,13 @@ CUtensorMap coefficient_map(const PlanCore& s, const void* base, uint32_t count)
 
 // the product planes (plane 0..P-1) of `count` workspaces: dims (column, prime, row, product),
 // so a box lands in shared memory as [row][prime][column]
-CUtensorMap residue_map(const PlanCore& s, const void* work, uint32_t count) {
+// Residue planes as (column, prime, row, product); a box of box_primes primes lands as
+// [row][box_primes][column] (primes past P read as zero).
+CUtensorMap residue_map(const PlanCore& s, const void* work, uint32_t count, uint32_t box_primes) {
     const uint32_t C = 1u << s.logC, R = 1u << s.logR, Gc = C < 8 ? C : 8;
     const cuuint64_t dims[4] = {C, s.P, R, count};
     const cuuint64_t strides[3] = {C * R * 4ull, C * 4ull, s.workspace_bytes};
-    const cuuint32_t box[4] = {Gc, s.P, R, 1};
+    const cuuint32_t box[4] = {Gc, box_primes, R, 1};
     return make_map(CU_TENSOR_MAP_DATA_TYPE_UINT32, work, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE);
 }
 
@@ -247,7 +249,7 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     PlanCrtWork w;
     std::memset(&w.map_res, 0, sizeof w.map_res);
     w.use_tma = (C * 4) % 16 == 0;  // rows of fewer than 4 columns cannot be described by a tensor map
-    if (w.use_tma) w.map_res = residue_map(s, work, count);
+    if (w.use_tma) w.map_res = residue_map(s, work, count, tc::kMaxPrimes);  // a constant row stride in the box
     w.work = work;
     w.out = c;
     w.ws_bstride = s.workspace_bytes / 4;
@@ -297,7 +299,7 @@ void launch_k3q(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K3Q shared memory");
     QuarticCrtWork w;
-    w.map_res = residue_map(s, work, count);
+    w.map_res = residue_map(s, work, count, s.P);
     w.out = c;
     w.io_bstride = size_t(s.n) * s.stride;
     w.consts = s.d_consts;

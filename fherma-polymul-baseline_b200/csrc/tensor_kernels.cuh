@@ -436,9 +436,10 @@ __device__ __forceinline__ void add1_carry(uint32_t& a, uint32_t b, uint32_t& cy
 // kCrtThreads = 256: all eight warps run the digit phase (the column stages of
 // the tile's (prime, column) pairs), warps 0-3 (the owners of the 128 TMEM
 // lanes) the per-coefficient epilogue.
-// An item's residues for every prime arrive by TMA (box: Gc columns x P primes x
-// R rows of u32, landing as [row][prime][column], so the 4 primes x 8 columns a
-// warp reads per row fall in 32 distinct banks); the next item's box is
+// An item's residues for every prime arrive by TMA (box: Gc columns x 64 primes x
+// R rows of u32, the primes past P zero-filled, landing as [row][prime][column]:
+// a constant row stride, and the 4 primes x 8 columns a warp reads per row fall
+// in 32 distinct banks); the next item's box is
 // requested as soon as this one has been turned into CRT digits, so it loads
 // during the MMA and the epilogue.  A-tile row m = r*Gc + c holds the digits of
 // coefficient (row r, column c): a warp's digit stores (8 columns x 4 primes)
@@ -492,7 +493,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         const CrtTarget t = w.target(it.x);
         if (!t.use_tma) return;
         const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
-        tc::mbar_expect_tx(&tma_bar, uint32_t(t.P * R * Gc) * 4u);
+        tc::mbar_expect_tx(&tma_bar, uint32_t(tc::kMaxPrimes * R * Gc) * 4u);  // the whole box, absent primes zero-filled
         tc::tma_load_4d(sR, t.map, it.y * Gc, 0, 0, t.mz, &tma_bar);
     };
     if (tid == 0 && begin < end) issue(begin);
@@ -533,7 +534,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             const int box = t.P * R * Gc;
             for (int q = tid; q < box; q += tc::kCrtThreads) {
                 const int c = q % Gc, i = (q / Gc) % t.P, r = q / (Gc * t.P);
-                sR[q] = t.work[size_t(i) * t.n + (size_t(r) << t.logC) + size_t(cg) * Gc + c];
+                sR[(r * tc::kMaxPrimes + i) * Gc + c] = t.work[size_t(i) * t.n + (size_t(r) << t.logC) + size_t(cg) * Gc + c];
             }
             __syncthreads();
         }
@@ -544,11 +545,10 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             constexpr int G = decltype(gconst)::value;
             const int gc = G ? G : Gc;
             const int i = G ? pr / G : pr / Gc, c = pr - i * gc;
-            const int P = t.P;
             const uint32_t p = s_p[i], two_p = 2 * p;
             uint32_t v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[r] = sR[(r * P + i) * gc + c];
+            for (int r = 0; r < R; ++r) v[r] = sR[(r * tc::kMaxPrimes + i) * gc + c];
             const uint2* tw = sTw + i * RT - 1;  // tw[k] = Psi_inv_rev[k], k >= 1
 #pragma unroll
             for (int s = LOGR - 1; s >= 1; --s) {
