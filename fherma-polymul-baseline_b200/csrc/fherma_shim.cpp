@@ -52,10 +52,17 @@ private:
             if (stop_) return;
             want_ = false;
             lock.unlock();
-            std::vector<uint32_t> v(words_);
+            std::vector<uint32_t> v;
+            try {
+                v.assign(words_, 0u);
+            } catch (...) {  // out of memory here: take() allocates on the caller's thread instead
+                v.clear();
+            }
             lock.lock();
-            spare_.swap(v);
-            ready_ = true;
+            if (v.size() == words_) {
+                spare_.swap(v);
+                ready_ = true;
+            }
         }
     }
     const size_t words_;
