@@ -304,3 +304,22 @@ def test_bad_device_pointers_are_refused(cuda, path):
         torch.cuda.synchronize()
         got = c.cpu().numpy().view(np.uint64)
         assert (got == oracle.rns_multiply(a.cpu().numpy().view(np.uint64), b.cpu().numpy().view(np.uint64), q)).all()
+
+
+@pytest.mark.parametrize("n", [1024, 32768])
+@pytest.mark.parametrize("qkind", ["random", "fherma"])
+def test_coefficients_that_are_multiples_of_q(cuda, path, n, qkind):
+    """a = 1 + X and b alternating (q-1)/2, (q+1)/2: every coefficient c_j, j >= 1, is
+    b_j + b_(j-1) = q as an integer, so its residue is 0 while its CRT value is not.
+    There the contraction's estimate of the quotient mod q can come out one low, and
+    only the final conditional subtraction of q brings the result back to 0."""
+    from tests.helpers import from_ints
+
+    rng = np.random.default_rng(700 + n)
+    q = random_q(rng, 868) if qkind == "random" else (1 << 868) - 11993087
+    a = from_ints([1, 1] + [0] * (n - 2), 14)
+    b = from_ints([(q - 1) // 2 if j % 2 == 0 else (q + 1) // 2 for j in range(n)], 14)
+    want = oracle.rns_multiply(a, b, q)
+    assert (want[1:] == 0).all()
+    with make_plan(path, n, q, 14) as p:
+        assert (p.multiply_host(a, b) == want).all()
