@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
         const int half = warp >> 2;  // primes 32*half .. 32*half + 31 of TMEM lanes 32(warp%4)..
         const int row = tid & 127;   // tile row m = this thread's TMEM lane
         const uint32_t taddr = tbase + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(128 * half);
-        const int ilo = 32 * half, ihi = min(P, ilo + 32);
+        const int ilo = 32 * half;
         uint32_t ph_mma = 0;
         for (int k = begin; k < end; ++k) {
             const TileItem it = w.item(k);
@@ -207,6 +207,8 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
             const int logC = LOGC ? LOGC : t.logC;
             const int C = 1 << logC, Gc = C < 8 ? C : 8;
             const size_t n = LOGC ? size_t(1) << (LOGR + LOGC) : size_t(t.n);
+            const int tP = t.P;  // this item's basis (at most the launch's P)
+            const int ihi = min(tP, ilo + 32);
             ok = tc::mbar_wait(&mma_full, ph_mma) && ok;
             ph_mma ^= 1u;
             tc::fence_after();
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
             tc::mbar_arrive(&tmem_empty);  // this thread's accumulator reads are complete
             tc::bar_sync(1, 256);
             // --- forward column stages of (prime, column) pairs, then the residue planes ---
-            const int pairs = P * Gc;
+            const int pairs = tP * Gc;
             for (int pr = tid; pr < pairs; pr += 256) {
                 const int i = Gc == 8 ? pr >> 3 : pr / Gc, c = pr - i * Gc;
                 const uint32_t p = spm[i].x, two_p = 2 * p;
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(tc::kWideThreads, 2) k1w_convert(const __grid_
                     for (int r = 0; r < R; ++r)
                         if (!(r & h)) ct_bfly(v[r], v[r + h], stw[i][(1 << s) + (r >> (LOGR - s)) - 1], p, two_p);
                 }
-                uint32_t* dst = t.res + (size_t(it.poly) * P + i) * n + size_t(it.cg) * Gc + c;
+                uint32_t* dst = t.res + (size_t(it.poly) * tP + i) * n + size_t(it.cg) * Gc + c;
                 const size_t rowstride = size_t(1) << logC;
 #pragma unroll
                 for (int r = 0; r < R; ++r, dst += rowstride) *dst = v[r];
