@@ -242,8 +242,12 @@ void launch_k3t(const PlanCore& s, const uint32_t* work, uint32_t* c, uint32_t c
     int ctas = s.sms * s.tune.crt_ctas_per_sm;
     if (ctas > items) ctas = items;
     const size_t smem = k3t_smem_bytes<LOGR>();
-    // the reduction mod q is a table row: the same kernel for a special-form q
+    // the reduction mod q is a table row: the same kernel for a special-form q; rows of 1024,
+    // 2048 or 4096 values (n = 16384 .. 65536) take a kernel with that row length built in
     auto kernel = k3t_crt<LOGR, W, PlanCrtWork>;
+    if (LOGR == 4 && s.logC == 10) kernel = k3t_crt<LOGR, W, PlanCrtWork, 10>;
+    if (LOGR == 4 && s.logC == 11) kernel = k3t_crt<LOGR, W, PlanCrtWork, 11>;
+    if (LOGR == 4 && s.logC == 12) kernel = k3t_crt<LOGR, W, PlanCrtWork, 12>;
     cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "K3T shared memory");
     PlanCrtWork w;

@@ -449,7 +449,9 @@ __device__ __forceinline__ void add1_carry(uint32_t& a, uint32_t b, uint32_t& cy
 // Dynamic shared memory (1024-aligned): A 2 x 16 KB (K = 256), B 2 x 16 KB,
 // residue box 64*R*8 words, inverse column twiddles 64*(R-1) uint2.
 // ---------------------------------------------------------------------------
-template <int LOGR, int W, class Work>
+// LOGC > 0: every item's rows hold 2^LOGC values (a plan's launch at a common ring size), so
+// the tile's column count and the output offsets are constants; 0: read from the item.
+template <int LOGR, int W, class Work, int LOGC = 0>
 __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_constant__ Work w, const PrimeConst* __restrict__ pcs,
                                                const uint2* __restrict__ tw_inv, uint32_t* __restrict__ err) {
     constexpr int R = 1 << LOGR;
@@ -492,7 +494,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
         const int2 it = w.item(k);
         const CrtTarget t = w.target(it.x);
         if (!t.use_tma) return;
-        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+        const int C = 1 << (LOGC ? LOGC : t.logC), Gc = C < 8 ? C : 8;
         tc::mbar_expect_tx(&tma_bar, uint32_t(tc::kMaxPrimes * R * Gc) * 4u);  // the whole box, absent primes zero-filled
         tc::tma_load_4d(sR, t.map, it.y * Gc, 0, 0, t.mz, &tma_bar);
     };
@@ -505,7 +507,8 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
     for (int k = begin; k < end; ++k) {
         const int2 it = w.item(k);
         const CrtTarget t = w.target(it.x);
-        const int C = 1 << t.logC, Gc = C < 8 ? C : 8;
+        const int logC = LOGC ? LOGC : t.logC;
+        const int C = 1 << logC, Gc = C < 8 ? C : 8;
         const int cg = it.y;
         if (t.crt_w != cur_w || t.P != cur_P) {  // the previous item's MMA is complete: B may be rewritten
             const uint4* src = reinterpret_cast<const uint4*>(t.crt_w);
@@ -680,7 +683,7 @@ __global__ void __launch_bounds__(tc::kCrtThreads, 2) k3t_crt(const __grid_const
             final_sub_q<W>(acc, s_q);
             const int rr = tid / Gc, cc = tid % Gc;
             if (rr < R) {
-                const size_t J = (size_t(rr) << t.logC) + size_t(cg) * Gc + cc;
+                const size_t J = (size_t(rr) << logC) + size_t(cg) * Gc + cc;
                 store_coef<W>(acc, t.out + J * t.stride, t.stride);
             }
         }
