@@ -67,6 +67,9 @@ def parse():
                     help="keep the default launch shapes instead of the autotuner's")
     ap.add_argument("--group", type=int, default=0,
                     help="products per launch group (default launch shapes otherwise; skips the autotuner)")
+    ap.add_argument("--conversion", choices=["whole", "groups"], default="whole",
+                    help="tensor path conversion for --ncu-case: whole (K1W, the whole basis per tile, "
+                         "the default) or groups (K1T, one group of 16 primes per tile)")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="K",
                     help="no timing: one batched call of K products in one launch group (one launch per pass), "
                          "for an ncu capture")
@@ -1026,12 +1029,12 @@ def run_ncu_case(args):
     c = torch.empty_like(a)
     plan = polymul.Plan(args.ring, q, coef_limbs=limbs, tensor=(args.path == "tensor"))
     # one batched call, all K products in one launch group (one launch per pass)
-    plan.set_tuning(group=args.ncu_case)
+    plan.set_tuning(group=args.ncu_case, conv_whole_basis=int(args.conversion == "whole"))
     plan.multiply_batch(a.data_ptr(), b.data_ptr(), c.data_ptr(), args.ncu_case)
     torch.cuda.synchronize()
     plan.close()
     print(f"ncu case: {args.ncu_case} products in one batched call, N={args.ring}, {args.bits}-bit q, "
-          f"path {args.path}")
+          f"path {args.path}, conversion {args.conversion}")
 
 
 def main():
