@@ -412,10 +412,8 @@ static __global__ void k2_rows_small(uint32_t* __restrict__ res, const PrimeCons
 // v (W+2 words) mod q, v < 2^(sbits+37); q has sbits bits and at most W words
 // (W is its word count rounded up to a multiple of 4, so sbits > 32(W-4));
 // mu_q = floor(2^(sbits+62) / q).  Leaves the canonical residue in v[0..W).
-// SMALLQ: the caller guarantees v < 2^32 q, so the quotient is one word and a
-// single W-word multiply-accumulate removes it.
 // ---------------------------------------------------------------------------
-template <int W, bool SMALLQ = false>
+template <int W>
 __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_t* __restrict__ q, uint64_t mu_q,
                                              int sbits) {
     // X = floor(v / 2^(sbits-26)) < 2^63; only words W-5 .. W+1 can hold it
@@ -436,12 +434,10 @@ __device__ __forceinline__ void reduce_mod_q(uint32_t (&v)[W + 2], const uint32_
     uint32_t t[W + 2], u[W + 2];
 #pragma unroll
     for (int k = 0; k < W + 2; ++k) t[k] = u[k] = 0;
-    crt_mac<W>(t, uint32_t(Q), qw);  // low 32 bits of Q times q
+    crt_mac<W>(t, uint32_t(Q), qw);        // low 32 bits of Q times q
+    crt_mac<W>(u, uint32_t(Q >> 32), qw);  // high bits (< 2^6) times q, subtracted one word up
     mp_sub<W + 2>(v, t);
-    if constexpr (!SMALLQ) {
-        crt_mac<W>(u, uint32_t(Q >> 32), qw);  // high bits (< 2^6) times q, subtracted one word up
-        mp_sub_hi<W>(v, u);
-    }
+    mp_sub_hi<W>(v, u);
     // [0, 2q) -> [0, q)
     uint32_t qq[W + 2];
 #pragma unroll
@@ -539,7 +535,7 @@ __device__ __forceinline__ void final_sub_q(uint32_t (&v)[W + 2], const uint32_t
 // (rows k = 0 .. 2P of k (-P mod q) mod q, W words each, 16-byte aligned) the
 // correction is one table row added instead of a W-word multiply-accumulate:
 // the same value mod q, and below v + q, inside reduce_mod_q's range.
-template <int W, int RED = kReduceEither, bool SMALLQ = false>
+template <int W, int RED = kReduceEither>
 __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t nearest, const uint32_t* s_q,
                                            uint64_t mu_q, int sbits, uint32_t delta, uint32_t* dst, int stride,
                                            const uint32_t* __restrict__ ktab = nullptr) {
@@ -565,12 +561,12 @@ __device__ __forceinline__ void crt_finish(uint32_t (&v)[W + 2], uint32_t neares
     if constexpr (RED == kReduceSpecial) {
         reduce_special<W>(v, s_q, sbits, delta);
     } else if constexpr (RED == kReduceGeneral) {
-        reduce_mod_q<W, SMALLQ>(v, s_q, mu_q, sbits);
+        reduce_mod_q<W>(v, s_q, mu_q, sbits);
     } else {
         if (delta)
             reduce_special<W>(v, s_q, sbits, delta);
         else
-            reduce_mod_q<W, SMALLQ>(v, s_q, mu_q, sbits);
+            reduce_mod_q<W>(v, s_q, mu_q, sbits);
     }
     store_coef<W>(v, dst, stride);
 }
