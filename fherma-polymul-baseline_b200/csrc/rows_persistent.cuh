@@ -113,7 +113,8 @@ __global__ void __launch_bounds__(k2p_threads(LOGC, KP), k2p_min_blocks(LOGC))
     for (int k = begin; k < end; ++k) {
         const RowItem it = w.item(k);
         const int i = it.i, r = it.r, pair = i * R + r;
-        if (pair != cur_pair) {  // twiddles are free: every thread passed the previous item's barrier
+        if (pair != cur_pair) {
+            if (cur_pair >= 0) __syncthreads();  // every thread is done with the previous pair's twiddles
             if (tid == 0) {
                 const uint2* gf = tw_fwd + size_t(i) * kNMax;
                 const uint2* gi = tw_inv + size_t(i) * kNMax;
@@ -147,8 +148,9 @@ __global__ void __launch_bounds__(k2p_threads(LOGC, KP), k2p_min_blocks(LOGC))
                 vb[(m << KP) + l] = sb[idx];
             }
         // the rows arrived unswizzled and the exchanges store swizzled: every thread
-        // has its values before any exchange store lands in this buffer
-        __syncthreads();
+        // has its values before any exchange store lands in this buffer (and a wait
+        // that gave up on any thread stops them all here)
+        if (__syncthreads_or(!ok)) break;
         // once every thread holds the last pass's values, the buffer takes the next item's rows
         auto hook = [&]() {
             tc::fence_smem_async();
@@ -164,9 +166,6 @@ __global__ void __launch_bounds__(k2p_threads(LOGC, KP), k2p_min_blocks(LOGC))
         for (int m = 0; m < (V >> KP); ++m)
 #pragma unroll
             for (int l = 0; l < (1 << KP); ++l) ga[pass_index<KP, false, LV>(tid, T, m, l, logd0)] = va[(m << KP) + l];
-        // this thread's shared-memory writes are ordered before the next bulk copy into this buffer
-        tc::fence_smem_async();
-        if (__syncthreads_or(!ok)) break;
     }
     // after a wait gave up (and the loop stopped): copies already requested land
     // before the CTA's shared memory goes away; no new copies were requested
